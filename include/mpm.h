@@ -1,0 +1,166 @@
+/*
+ * mpm.h -- C ABI of libmpm.so, the B200 (sm_100a) implementation of the
+ * MPM snow simulation step of luoluobuli/WebGPU-MPM-based-Snow-Simulation.
+ *
+ * The library keeps the reference's data contracts:
+ *   - particles are the 192-byte ParticleData records of
+ *     src/lib/gpu/shaderPrelude/mpmOps.wgsl:1-12 (GpuMpmBufferManager.ts:22-26);
+ *   - step parameters arrive as the reference's 37,376-byte uniform block
+ *     (src/lib/gpu/shaderPrelude/uniforms.wgsl:8-56,
+ *     src/lib/gpu/uniforms/GpuUniformsBufferManager.ts:15-182), plus an
+ *     extension struct for the constants the WGSL hard-codes;
+ *   - the collider is the reference's packed u32 buffer and 32-byte BVH nodes
+ *     (src/lib/gpu/collider/GpuColliderBufferManager.ts:96-220,
+ *     src/lib/gpu/mpm/colliderPrelude.wgsl:1-27).
+ *
+ * Conventions: every function returns an int status (MPM_OK = 0, negative =
+ * error; mpm_last_error() gives the message).  No exception crosses the ABI.
+ * A handle is not thread-safe; all device work is ordered on the handle's
+ * CUDA stream and asynchronous unless stated.  Scenes: a handle advances
+ * one or more independent scenes in the same launches; scene s owns the
+ * particle records [first, first+count) given by mpm_set_scene_range().
+ */
+#ifndef MPM_H
+#define MPM_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_UNIFORMS_BYTES 37376u
+#define MPM_PARTICLE_BYTES 192u
+#define MPM_BVH_NODE_BYTES 32u
+
+#define MPM_OK 0
+#define MPM_ERR_ARG (-1)
+#define MPM_ERR_CUDA (-2)
+#define MPM_ERR_CAPACITY (-3)
+#define MPM_ERR_STATE (-4)
+#define MPM_ERR_DEVICE_STATUS (-5)
+
+/* Simulation methods (src/lib/gpu/GpuSimulationMethod.ts:1-4). */
+#define MPM_METHOD_EXPLICIT 0
+#define MPM_METHOD_PBMPM 1
+
+/* Device status bits, sticky until mpm_clear_status(). */
+#define MPM_STATUS_HASH_FULL      0x1u  /* tile hash table ran out of probes */
+#define MPM_STATUS_TILE_OVERFLOW  0x2u  /* more occupied tiles than max_tiles */
+#define MPM_STATUS_BVH_STACK      0x4u  /* BVH traversal dropped children (stack of 32 full) */
+#define MPM_STATUS_SCENE_RANGE    0x8u  /* a particle index belongs to no scene */
+#define MPM_STATUS_MLP_FALLBACK   0x10u /* learned plasticity fell back to the exact map */
+
+typedef struct MpmHandle MpmHandle;
+
+typedef struct MpmConfig {
+    uint32_t max_particles;  /* capacity of the particle buffer, all scenes */
+    uint32_t max_scenes;     /* 1 for a single scene */
+    uint32_t max_tiles;      /* occupied grid tiles per substep (0: derived) */
+    uint32_t hash_capacity;  /* tile hash slots, rounded up to a power of two (0: derived) */
+    uint32_t tile_edge;      /* grid tile edge in cells: 8 or 16 (0: 16) */
+    int32_t device;          /* CUDA device ordinal */
+    void* stream;            /* cudaStream_t to order work on, or NULL for a private stream */
+} MpmConfig;
+
+/* Constants the reference hard-codes in WGSL, per scene.  mpm_default_params
+ * fills the reference values (cited per field). */
+typedef struct MpmParams {
+    float gravity[3];            /* gridUpdate.cs.wgsl:43, pbmpm.wgsl:101: (0,0,-9.81) */
+    float youngs_modulus;        /* stressTensorOps.wgsl:1: 1.4e5 */
+    float poissons_ratio;        /* stressTensorOps.wgsl:2: 0.2 */
+    float hardening_explicit;    /* stressTensorOps.wgsl:44: 5 */
+    float hardening_pbmpm;       /* pbmpm.wgsl:35: 20 */
+    float theta_c;               /* plasticityOps.wgsl:18: 2.5e-2 */
+    float theta_s;               /* plasticityOps.wgsl:19: 7.5e-3 */
+    float density;               /* particleToGrid.cs.wgsl:36: 400 */
+    uint32_t n_iter;             /* GpuMpmPipelineManager.ts:445: 3 */
+    float force_divisor;         /* pbmpm.wgsl:137: 3 */
+    uint32_t boundary_mode;      /* 0 reference particle reflect; 1 adds grid sticky ground + slip walls */
+    float restitution;           /* integrateParticles.wgsl:34: -0.5 */
+    uint32_t bc_cells;           /* boundary_mode 1: boundary layer width, cells (2) */
+    uint32_t ground_axis;        /* boundary_mode 1: sticky plane at grid min of this axis (2) */
+    float collider_margin;       /* colliderPrelude.wgsl:158: 0.05 */
+    float collider_surface_margin; /* colliderPrelude.wgsl:297,351: 0.05 */
+    float collider_threshold;    /* colliderPrelude.wgsl:330: 0.05 */
+    float collider_friction;     /* colliderPrelude.wgsl:308: 0.1 */
+    float collider_vel_scale;    /* colliderPrelude.wgsl:294: 0.2 */
+    float pbmpm_blend;           /* pbmpm.wgsl:26: 0.95 */
+    float pbmpm_volume_exponent; /* pbmpm.wgsl:23: -0.3333333 */
+} MpmParams;
+
+/* ---- lifetime ------------------------------------------------------ */
+int mpm_default_params(MpmParams* out);
+/* Allocates every device buffer up front; nothing is allocated per step. */
+int mpm_create(const MpmConfig* cfg, MpmHandle** out);
+int mpm_destroy(MpmHandle* h);
+const char* mpm_last_error(const MpmHandle* h);
+
+/* ---- parameters (GpuUniformsBufferManager.ts:54-182) ---------------- */
+/* Accepts the reference uniform block verbatim (n >= 544 bytes are read:
+ * the fields the step uses lie below the collider-object array). */
+int mpm_set_uniforms(MpmHandle* h, uint32_t scene, const void* bytes, size_t n);
+int mpm_set_params(MpmHandle* h, uint32_t scene, const MpmParams* p);
+/* Scene s owns particle records [first, first + count); scenes must tile
+ * [0, n_particles) in increasing order. */
+int mpm_set_scene_range(MpmHandle* h, uint32_t scene, uint32_t first, uint32_t count);
+int mpm_set_scene_count(MpmHandle* h, uint32_t n_scenes);
+
+/* ---- particles (GpuMpmBufferManager.ts:22-26) ---------------------- */
+/* Copies n 192-byte records into the library buffer (src on host or device). */
+int mpm_set_particles(MpmHandle* h, const void* src, uint32_t n, int src_is_device);
+int mpm_get_particles(MpmHandle* h, void* dst, uint32_t n, int dst_is_device);
+/* Zero-copy: the step reads and writes the caller's device buffer of n records. */
+int mpm_bind_particles_device(MpmHandle* h, void* dptr, uint32_t n);
+void* mpm_particles_device_ptr(MpmHandle* h);
+
+/* ---- collider (GpuColliderBufferManager.ts:61-220) ------------------ */
+/* data: [reordered indices (num_indices u32) | vertices f32x3 | ...];
+ * nodes: n_nodes 32-byte BVH nodes.  Host pointers; copied to the device. */
+int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* data, size_t words,
+                     uint32_t num_indices, const void* nodes, uint32_t n_nodes);
+/* Host-side BVH build in the reference format (GpuColliderBufferManager.ts:222-350):
+ * median split on the longest axis, leaves of <= 4 triangles, pre-order nodes.
+ * nodes_out needs room for 2*n_tris+1 nodes; tri_order_out for n_tris. */
+int mpm_build_bvh(const float* vertices, uint32_t n_vertices, const uint32_t* indices,
+                  uint32_t n_indices, void* nodes_out, uint32_t* tri_order_out, uint32_t* n_nodes_out);
+
+/* ---- the step (GpuMpmPipelineManager.ts:327-521) ------------------- */
+/* Enqueues n_substeps substeps of `method` on the handle's stream. */
+int mpm_step(MpmHandle* h, int method, uint32_t n_substeps);
+/* The reference's two entry points, one substep each
+ * (GpuMpmPipelineManager.ts:327 addExplicitMpmDispatches, :431 addPbmpmDispatches).
+ * n_particles must equal the bound particle count. */
+int mpm_add_explicit_mpm_dispatches(MpmHandle* h, uint32_t n_particles);
+int mpm_add_pbmpm_dispatches(MpmHandle* h, uint32_t n_particles);
+/* Waits for the stream; returns MPM_ERR_DEVICE_STATUS if a status bit is set. */
+int mpm_sync(MpmHandle* h, uint32_t* status_out);
+int mpm_clear_status(MpmHandle* h);
+
+/* ---- inspection ----------------------------------------------------- */
+/* Runs one substep only up to its first particle-to-grid transfer (for grid
+ * parity checks); the particle buffer keeps its input values. */
+int mpm_step_p2g_only(MpmHandle* h, int method);
+/* Dense copy of scene `scene`'s grid, [res_z][res_y][res_x][4] i32 (mass,
+ * momentum x, y, z) in the reference fixed-point encoding; cells no particle
+ * reaches are 0.  apply_grid_update = 1 reproduces the explicit grid update
+ * (gridUpdate.cs.wgsl:15-53), i.e. the reference buffers after a full
+ * explicit substep.  Synchronous. */
+int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_update,
+                       int32_t* out_host, size_t n_cells);
+/* Number of occupied tiles and binned particles of the last substep (synchronous). */
+int mpm_get_counts(MpmHandle* h, uint32_t* n_tiles, uint32_t* n_binned);
+/* Per-kernel timing: when enabled, each launch of a substep is bracketed by
+ * CUDA events on the handle's stream; mpm_kernel_times returns the summed
+ * milliseconds and launch counts per kernel id since the last reset. */
+int mpm_enable_kernel_timing(MpmHandle* h, int enable);
+int mpm_kernel_times(MpmHandle* h, float* ms_out, uint32_t* launches_out, uint32_t n_kernels);
+const char* mpm_kernel_name(uint32_t kernel_id);
+uint32_t mpm_kernel_count(void);
+/* Captures each substep into a CUDA graph (default on). */
+int mpm_use_graphs(MpmHandle* h, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,185 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU oracle (liboracle.so,
+built from mpm_oracle.c / bvh_oracle.c by oracle/Makefile).
+
+The oracle restates the reference MPM step (WGSL under src/lib/gpu/mpm/ and
+src/lib/gpu/shaderPrelude/, scheduled by GpuMpmPipelineManager.ts:327-521).
+Parity status: UNPINNED -- the reference ships no golden vectors and its
+WGSL cannot run here.  Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg may import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+UNIFORMS_BYTES = 37376
+
+
+def build(force: bool = False) -> str:
+    srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "Makefile")]
+    if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
+        subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return LIB
+
+
+class OrExt(C.Structure):
+    _fields_ = [
+        ("gravity", C.c_float * 3), ("youngs_modulus", C.c_float), ("poissons_ratio", C.c_float),
+        ("hardening_explicit", C.c_float), ("hardening_pbmpm", C.c_float), ("theta_c", C.c_float),
+        ("theta_s", C.c_float), ("density", C.c_float), ("n_iter", C.c_uint32), ("force_divisor", C.c_float),
+        ("boundary_mode", C.c_uint32), ("restitution", C.c_float), ("bc_cells", C.c_uint32),
+        ("ground_axis", C.c_uint32), ("collider_margin", C.c_float), ("collider_surface_margin", C.c_float),
+        ("collider_threshold", C.c_float), ("collider_friction", C.c_float), ("collider_vel_scale", C.c_float),
+        ("pbmpm_blend", C.c_float), ("pbmpm_volume_exponent", C.c_float),
+    ]
+
+
+class OrCollider(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("data_words", C.c_uint32), ("nodes", C.c_void_p), ("n_nodes", C.c_uint32)]
+
+
+D_DTYPE = np.dtype([("pos", "<3f8"), ("vel", "<3f8"), ("mass", "<f8"), ("Fe", "<9f8"), ("Fp", "<9f8"),
+                    ("dxp", "<3f8"), ("D", "<9f8")])
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        L = _lib
+        V, U32, I32 = C.c_void_p, C.c_uint32, C.c_int
+        sig = {
+            "or_default_ext": (None, [V]),
+            "orf_create": (V, [U32, U32, U32]), "orf_destroy": (None, [V]), "orf_status": (U32, [V]),
+            "orf_set_threads": (None, [I32]),
+            "orf_step": (I32, [V, V, V, V, U32, V, I32, I32]), "orf_dense_grid": (I32, [V, V, V]),
+            "orf_n_blocks": (U32, [V]),
+            "ord_create": (V, [U32, U32, U32]), "ord_destroy": (None, [V]), "ord_status": (U32, [V]),
+            "ord_step": (I32, [V, V, V, V, U32, V, I32, I32]), "ord_dense_grid": (I32, [V, V, V]),
+            "or_hash3": (U32, [U32, U32, U32]), "or_expf": (C.c_float, [C.c_float]),
+            "or_powf": (C.c_float, [C.c_float, C.c_float]), "or_f2i": (C.c_int32, [C.c_float]),
+            "orf_inverse": (None, [V, V]), "orf_polar": (None, [V, V]), "orf_det": (C.c_float, [V]),
+            "orf_plasticity": (None, [V, V, V]),
+            "or_bvh_build": (U32, [V, U32, V, U32, V, V]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def make_ext(params: dict) -> OrExt:
+    e = OrExt()
+    lib().or_default_ext(C.byref(e))
+    for k, v in params.items():
+        if k == "gravity":
+            e.gravity[:] = [float(x) for x in v]
+        else:
+            setattr(e, k, v)
+    return e
+
+
+def bvh_build(vertices, indices):
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    nt = i.size // 3
+    nodes = np.zeros((2 * nt + 1, 8), np.uint32)
+    order = np.zeros(max(nt, 1), np.uint32)
+    n = lib().or_bvh_build(v.ctypes.data, v.size // 3, i.ctypes.data, i.size, nodes.ctypes.data, order.ctypes.data)
+    return nodes[:n].copy(), order[:nt].copy()
+
+
+def collider_buffers(vertices, indices):
+    """Packed [indices in BVH order | vertices] and nodes, built by the oracle."""
+    nodes, order = bvh_build(vertices, indices)
+    tri = np.asarray(indices, np.uint32).reshape(-1, 3)
+    data = np.concatenate([tri[order].reshape(-1), np.asarray(vertices, np.float32).reshape(-1).view(np.uint32)])
+    return np.ascontiguousarray(data, np.uint32), nodes
+
+
+class Oracle:
+    """One oracle context (f32 with fixed-point grid, or f64)."""
+
+    def __init__(self, n_particles: int, max_blocks: int = 200000, hash_size: int = 2000003, fp64: bool = False,
+                 threads: int = 0):
+        self.fp64 = fp64
+        L = lib()
+        if threads:
+            L.orf_set_threads(threads)
+        self.ctx = (L.ord_create if fp64 else L.orf_create)(hash_size, max_blocks, max(n_particles, 1))
+        if not self.ctx:
+            raise MemoryError("oracle context allocation failed")
+        self._col = None
+
+    def close(self):
+        if self.ctx:
+            (lib().ord_destroy if self.fp64 else lib().orf_destroy)(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_collider(self, vertices, indices):
+        if vertices is None:
+            self._col = None
+            return
+        data, nodes = collider_buffers(vertices, indices)
+        self._col_keep = (data, nodes)
+        self._col = OrCollider(data.ctypes.data, data.size, nodes.ctypes.data, nodes.shape[0])
+
+    def step(self, uniforms: bytes, params: dict, particles: np.ndarray, method: int, stop_after: int = 0) -> None:
+        """Advances `particles` in place (f32 records, or D_DTYPE for fp64)."""
+        ub = np.frombuffer(bytes(uniforms).ljust(UNIFORMS_BYTES, b"\0"), np.uint8)
+        ext = make_ext(params)
+        assert particles.flags["C_CONTIGUOUS"]
+        fn = lib().ord_step if self.fp64 else lib().orf_step
+        col = C.byref(self._col) if self._col is not None else None
+        rc = fn(self.ctx, ub.ctypes.data, C.byref(ext), particles.ctypes.data, particles.shape[0], col, method,
+                stop_after)
+        if rc != 0:
+            raise RuntimeError(f"oracle step failed: {rc}")
+
+    def status(self) -> int:
+        return (lib().ord_status if self.fp64 else lib().orf_status)(self.ctx)
+
+    def dense_grid(self, uniforms: bytes) -> np.ndarray:
+        ub = np.frombuffer(bytes(uniforms).ljust(UNIFORMS_BYTES, b"\0"), np.uint8)
+        res = np.frombuffer(ub[208:220].tobytes(), "<u4")
+        out = np.zeros((res[2], res[1], res[0], 4), np.float64 if self.fp64 else np.int32)
+        (lib().ord_dense_grid if self.fp64 else lib().orf_dense_grid)(self.ctx, ub.ctypes.data, out.ctypes.data)
+        return out
+
+
+def to_fp64(records: np.ndarray) -> np.ndarray:
+    d = np.zeros(records.shape[0], D_DTYPE)
+    d["pos"] = records["pos"]
+    d["vel"] = records["vel"]
+    d["mass"] = records["mass"]
+    d["Fe"] = records["Fe"][:, :, :3].reshape(-1, 9)
+    d["Fp"] = records["Fp"][:, :, :3].reshape(-1, 9)
+    d["dxp"] = records["dxp"]
+    d["D"] = records["D"][:, :, :3].reshape(-1, 9)
+    return d
+
+
+def aggregates(pos, vel, mass, Fp9):
+    """Centre of mass, total momentum and mean J_p = det(F_p) (f64)."""
+    m = np.asarray(mass, np.float64)
+    pos = np.asarray(pos, np.float64)
+    vel = np.asarray(vel, np.float64)
+    F = np.asarray(Fp9, np.float64).reshape(-1, 3, 3)
+    com = (pos * m[:, None]).sum(0) / m.sum()
+    mom = (vel * m[:, None]).sum(0)
+    jp = np.linalg.det(F).mean()
+    return com, mom, jp

@@ -1,0 +1,137 @@
+"""Parity of the CUDA step (through the C ABI) with the CPU oracle.
+
+Bar: the fixed-point grid is compared bit for bit, and so are the particle
+fields, because the CUDA path evaluates the oracle's canonical operation
+order (no FMA contraction, IEEE division, the same f64 exp/log).  Where a
+test states a tolerance it is the relative bound 1e-5 on single-step fields.
+"""
+import numpy as np
+import pytest
+
+from helpers import GpuScene, bits_equal, compare_states, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(pkg, **kw):
+    return pkg.scenes.parity_scene(**kw)
+
+
+@pytest.mark.parametrize("kind,interaction", [("explicit", False), ("pbmpm", False), ("pbmpm", True)])
+def test_p2g_grid_bit_exact(gpu, oracle_mod, kind, interaction):
+    spec = _scene(gpu, kind=kind, interaction=interaction)
+    g = GpuScene(gpu, spec)
+    assert g.p2g_only() == 0
+    grid_gpu = g.grid()
+    o, _ = run_oracle(oracle_mod, spec, stop_after=1)
+    grid_ref = o.dense_grid(spec.uniforms.bytes())
+    assert np.count_nonzero(grid_ref[..., 0]) > 100
+    assert np.array_equal(grid_gpu, grid_ref), f"{np.count_nonzero(grid_gpu != grid_ref)} cells differ"
+    g.close()
+
+
+@pytest.mark.parametrize("kind,collider,interaction", [
+    ("explicit", False, False), ("explicit", True, False), ("pbmpm", False, False), ("pbmpm", True, True)])
+def test_one_step_bit_exact(gpu, oracle_mod, kind, collider, interaction):
+    spec = _scene(gpu, kind=kind, with_collider=collider, interaction=interaction)
+    g = GpuScene(gpu, spec)
+    assert g.step(1) == 0
+    got = g.particles()
+    o, want = run_oracle(oracle_mod, spec, n_steps=1)
+    compare_states(got, want)
+    grid_gpu = g.grid(apply_update=(kind == "explicit"))
+    grid_ref = o.dense_grid(spec.uniforms.bytes())
+    assert np.array_equal(grid_gpu, grid_ref)
+    g.close()
+
+
+@pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
+def test_multi_step_bit_exact_and_aggregates(gpu, oracle_mod, kind):
+    spec = _scene(gpu, kind=kind, with_collider=True, n_side=12)
+    n = 20
+    g = GpuScene(gpu, spec)
+    assert g.step(n) == 0
+    got = g.particles()
+    _, want = run_oracle(oracle_mod, spec, n_steps=n)
+    compare_states(got, want)
+    # aggregates against the f64 oracle (error statement, loose bound)
+    _, w64 = run_oracle(oracle_mod, spec, n_steps=n, fp64=True)
+    c32 = oracle_mod.aggregates(got["pos"], got["vel"], got["mass"], got["Fp"][:, :, :3].reshape(-1, 9))
+    c64 = oracle_mod.aggregates(w64["pos"], w64["vel"], w64["mass"], w64["Fp"])
+    assert np.allclose(c32[0], c64[0], rtol=1e-3, atol=1e-3)
+    g.close()
+
+
+@pytest.mark.parametrize("n", [1, 7, 255, 257])
+def test_small_and_ragged_counts(gpu, oracle_mod, n):
+    spec = _scene(gpu, kind="explicit", n_side=8)
+    spec.particles = spec.particles[:n].copy()
+    g = GpuScene(gpu, spec)
+    assert g.step(2) == 0
+    _, want = run_oracle(oracle_mod, spec, n_steps=2)
+    compare_states(g.particles(), want)
+    g.close()
+
+
+def test_tile_edges_agree(gpu, oracle_mod):
+    spec = _scene(gpu, kind="pbmpm", with_collider=True)
+    outs = []
+    for e in (8, 16):
+        g = GpuScene(gpu, spec, tile_edge=e)
+        assert g.step(3) == 0
+        outs.append(g.particles())
+        g.close()
+    compare_states(outs[0], outs[1])
+
+
+def test_graph_and_eager_agree(gpu):
+    spec = _scene(gpu, kind="explicit", with_collider=True)
+    outs = []
+    for use_graphs in (True, False):
+        g = GpuScene(gpu, spec, use_graphs=use_graphs)
+        assert g.step(4) == 0
+        outs.append(g.particles())
+        g.close()
+    compare_states(outs[0], outs[1])
+
+
+def test_particles_outside_domain(gpu, oracle_mod):
+    """Particles below the grid minimum and far outside it: the oracle and the
+    GPU both reflect them back to the boundary."""
+    spec = _scene(gpu, kind="explicit", n_side=8)
+    p = spec.particles
+    p["pos"][0] = [-0.01, 0.5, 0.5]
+    p["pos"][1] = [0.5, -3.0, 0.5]
+    p["pos"][2] = [0.5, 0.5, 7.0]
+    g = GpuScene(gpu, spec)
+    assert g.step(1) == 0
+    _, want = run_oracle(oracle_mod, spec, n_steps=1)
+    compare_states(g.particles(), want)
+    g.close()
+
+
+def test_tile_overflow_reports_status(gpu):
+    """Capacity overflow sets a status bit instead of dropping work silently."""
+    spec = gpu.scenes.c0_explicit_snow(n_side=16)
+    g = GpuScene(gpu, spec, tile_edge=8, max_tiles=2)
+    with pytest.raises(gpu.MpmError) as ei:
+        g.step(1)
+    assert ei.value.status & 0x2
+    g.close()
+
+
+def test_permutation_invariance(gpu):
+    """Results per particle do not depend on the record order."""
+    spec = _scene(gpu, kind="pbmpm", with_collider=True)
+    g = GpuScene(gpu, spec)
+    assert g.step(2) == 0
+    a = g.particles()
+    g.close()
+    perm = np.random.default_rng(5).permutation(spec.particles.shape[0])
+    spec.particles = spec.particles[perm].copy()
+    g = GpuScene(gpu, spec)
+    assert g.step(2) == 0
+    b = g.particles()
+    g.close()
+    inv = np.argsort(perm)
+    compare_states(b[inv], a)

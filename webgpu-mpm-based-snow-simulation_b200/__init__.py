@@ -1,0 +1,20 @@
+"""B200-native (sm_100a) MPM snow simulation step.
+
+Drop-in for the step of luoluobuli/WebGPU-MPM-based-Snow-Simulation: the
+reference's 192-byte particle records and uniform block go in, the same
+records come out.  Compute runs in libmpm.so (include/mpm.h); this package is
+the host-side mirror of the reference's TypeScript managers plus scene
+generators.
+"""
+from . import _lib, layout, scenes
+from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams, default_params, load
+from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
+from .pipeline import (GpuColliderBufferManager, GpuMpmBufferManager, GpuMpmPipelineManager,
+                       GpuSimulationMethodType, build_bvh, kernel_names)
+
+__all__ = [
+    "METHOD_EXPLICIT", "METHOD_PBMPM", "MpmConfig", "MpmError", "MpmParams", "default_params", "load",
+    "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
+    "GpuMpmBufferManager", "GpuMpmPipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
+    "layout", "scenes",
+]

@@ -1,0 +1,790 @@
+// mpm_api.cu -- host engine behind the C ABI of include/mpm.h.
+//
+// The handle owns every device buffer (allocated in mpm_create), the
+// per-scene parameter table and the CUDA graphs of the two substep
+// schedules.  A substep is a fixed launch sequence on one stream; counts
+// that change from step to step (occupied tiles, binned particles) stay on
+// the device and the kernels read them there, so the sequence is graph-
+// capturable and needs no host round trip.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm.h"
+#include "mpm_engine.cuh"
+
+namespace mpm {
+template <int E> cudaError_t configure_tile_kernels(int* blocks_per_sm);
+template <int E> cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_tiles, uint32_t scene,
+                                           int apply, int4* out);
+}  // namespace mpm
+
+using namespace mpm;
+
+static const char* kKernelNames[K_COUNT] = {
+    "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
+    "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense"};
+
+struct TimedLaunch {
+    uint32_t kid;
+    cudaEvent_t a, b;
+};
+
+struct SceneHost {
+    SceneDev dev;
+    MpmParams params;
+    uint8_t uni[MPM_UNIFORMS_BYTES];
+    bool have_uniforms = false;
+    uint32_t* col_data = nullptr;
+    uint32_t* bvh = nullptr;
+};
+
+struct MpmHandle {
+    MpmConfig cfg{};
+    int device = 0;
+    int n_sms = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    uint32_t tile_edge = 16;
+    uint32_t cap = 0;
+    uint32_t max_tiles = 0;
+
+    float4* particles = nullptr;
+    bool own_particles = true;
+    uint32_t n_particles = 0;
+    uint32_t* order[2] = {nullptr, nullptr};
+    int order_parity = 0;
+    bool order_valid = false;
+    uint32_t* bin_slot = nullptr;
+    uint32_t* bin_rank = nullptr;
+    unsigned long long* keys = nullptr;
+    uint32_t* slot_count = nullptr;
+    uint32_t* slot_off = nullptr;
+    uint32_t* slot_st = nullptr;
+    unsigned long long* st_key = nullptr;
+    uint32_t* st_slot = nullptr;
+    uint32_t* st_begin = nullptr;
+    uint32_t* st_count = nullptr;
+    uint32_t* chunk_nst = nullptr;
+    uint32_t* chunk_np = nullptr;
+    int4* tiles[2] = {nullptr, nullptr};
+    int last_tiles = 0;
+    SceneDev* d_scenes = nullptr;
+    uint32_t* d_scene_first = nullptr;
+    Counters* counters = nullptr;
+
+    std::vector<SceneHost> scenes;
+    uint32_t n_scenes = 1;
+    std::vector<uint32_t> scene_first;  // n_scenes + 1
+    bool scenes_dirty = true;
+
+    int blocks_per_sm[K_COUNT] = {0};
+
+    bool use_graphs = true;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [method][parity]
+    uint64_t graph_sig[2][2] = {{0, 0}, {0, 0}};
+
+    bool timing = false;
+    std::vector<TimedLaunch> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double kms[K_COUNT] = {0};
+    uint32_t kcount[K_COUNT] = {0};
+};
+
+static int fail(MpmHandle* h, int code, const char* fmt, ...) {
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return code;
+}
+
+#define CK(h, expr)                                                                              \
+    do {                                                                                         \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess) return fail((h), MPM_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+static uint32_t next_pow2(uint32_t v) {
+    uint32_t p = 1;
+    while (p < v && p < 0x80000000u) p <<= 1;
+    return p;
+}
+
+extern "C" int mpm_default_params(MpmParams* p) {
+    if (!p) return MPM_ERR_ARG;
+    std::memset(p, 0, sizeof(*p));
+    p->gravity[0] = 0.0f; p->gravity[1] = 0.0f; p->gravity[2] = -9.81f;
+    p->youngs_modulus = 1.4e5f;
+    p->poissons_ratio = 0.2f;
+    p->hardening_explicit = 5.0f;
+    p->hardening_pbmpm = 20.0f;
+    p->theta_c = 2.5e-2f;
+    p->theta_s = 7.5e-3f;
+    p->density = 400.0f;
+    p->n_iter = 3;
+    p->force_divisor = 3.0f;
+    p->boundary_mode = 0;
+    p->restitution = -0.5f;
+    p->bc_cells = 2;
+    p->ground_axis = 2;
+    p->collider_margin = 0.05f;
+    p->collider_surface_margin = 0.05f;
+    p->collider_threshold = 0.05f;
+    p->collider_friction = 0.1f;
+    p->collider_vel_scale = 0.2f;
+    p->pbmpm_blend = 0.95f;
+    p->pbmpm_volume_exponent = -0.3333333f;
+    return MPM_OK;
+}
+
+static float rdf(const uint8_t* u, size_t off) { float f; std::memcpy(&f, u + off, 4); return f; }
+static uint32_t rdu(const uint8_t* u, size_t off) { uint32_t v; std::memcpy(&v, u + off, 4); return v; }
+
+// Fill the device scene record from the uniform block
+// (shaderPrelude/uniforms.wgsl:8-56 offsets) and the extension parameters.
+static void build_scene_dev(SceneHost& s) {
+    SceneDev& d = s.dev;
+    const uint8_t* u = s.uni;
+    const MpmParams& e = s.params;
+    const uint32_t* col = d.col_data;
+    const uint32_t* bvh = d.bvh;
+    uint32_t col_words = d.col_words, n_nodes = d.n_nodes, p_first = d.p_first, p_count = d.p_count;
+    uint32_t c_nidx_override = d.c_nidx;
+    std::memset(&d, 0, sizeof(d));
+    d.dt = rdf(u, 0);
+    d.scale = rdf(u, 4);
+    for (int i = 0; i < 3; i++) {
+        d.gmin[i] = rdf(u, 16 + 4 * i);
+        d.gmax[i] = rdf(u, 32 + 4 * i);
+        d.res[i] = (int32_t)rdu(u, 208 + 4 * i);
+        d.cmin[i] = rdf(u, 224 + 4 * i);
+        d.cmax[i] = rdf(u, 240 + 4 * i);
+        d.cvel[i] = rdf(u, 320 + 4 * i);
+        d.cd[i] = rdf(u, 352 + 4 * i);
+        d.ipos[i] = rdf(u, 496 + 4 * i);
+    }
+    for (int i = 0; i < 16; i++) {
+        d.xf[i] = rdf(u, 256 + 4 * i);
+        d.xfi[i] = rdf(u, 432 + 4 * i);
+    }
+    d.c_nidx = rdu(u, 348);
+    if (d.c_nidx == 0u) d.c_nidx = c_nidx_override;
+    d.c_nobj = rdu(u, 364);
+    d.istr = rdf(u, 508);
+    d.irad = rdf(u, 512);
+    d.iact = rdu(u, 516);
+    d.imode = rdu(u, 520);
+    for (int i = 0; i < 3; i++) d.g[i] = e.gravity[i];
+    // WGSL folds these constant expressions in abstract (f64) precision and
+    // rounds once (stressTensorOps.wgsl:5-6, plasticityOps.wgsl:18-19,
+    // particleToGrid.cs.wgsl:37).
+    double E = e.youngs_modulus, nu = e.poissons_ratio;
+    d.mu0 = (float)(E / (2.0 * (1.0 + nu)));
+    d.la0 = (float)(E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+    d.xi_e = e.hardening_explicit;
+    d.xi_p = e.hardening_pbmpm;
+    d.smin = (float)(1.0 - (double)e.theta_c);
+    d.smax = (float)(1.0 + (double)e.theta_s);
+    d.inv_rho = (float)(1.0 / (double)e.density);
+    d.n_iter = e.n_iter;
+    d.fdiv = e.force_divisor;
+    d.bmode = e.boundary_mode;
+    d.rest = e.restitution;
+    d.bc = (int32_t)e.bc_cells;
+    d.gaxis = e.ground_axis > 2 ? 2 : e.ground_axis;
+    d.cmargin = e.collider_margin;
+    d.csurf = e.collider_surface_margin;
+    d.cthr = e.collider_threshold;
+    d.cfric = e.collider_friction;
+    d.cvs = e.collider_vel_scale;
+    d.blend = e.pbmpm_blend;
+    d.vexp = e.pbmpm_volume_exponent;
+    d.p_first = p_first;
+    d.p_count = p_count;
+    d.col_data = col;
+    d.bvh = bvh;
+    d.col_words = col_words;
+    d.n_nodes = n_nodes;
+    // power-of-two fixed-point scale: x / s == x * (1/s) exactly
+    uint32_t sb;
+    std::memcpy(&sb, &d.scale, 4);
+    int ex = (int)((sb >> 23) & 0xff) - 127;
+    d.scale_is_pow2 = ((sb & 0x807fffffu) == 0u && ex >= -100 && ex <= 100) ? 1u : 0u;
+    d.inv_scale = d.scale_is_pow2 ? (float)(1.0 / (double)d.scale) : 0.0f;
+}
+
+static void destroy_graphs(MpmHandle* h) {
+    for (int m = 0; m < 2; m++)
+        for (int p = 0; p < 2; p++) {
+            if (h->graph[m][p]) cudaGraphExecDestroy(h->graph[m][p]);
+            h->graph[m][p] = nullptr;
+            h->graph_sig[m][p] = 0;
+        }
+}
+
+extern "C" int mpm_destroy(MpmHandle* h) {
+    if (!h) return MPM_ERR_ARG;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    destroy_graphs(h);
+    for (auto& t : h->pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    for (auto e : h->event_pool) cudaEventDestroy(e);
+    void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
+                    h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
+                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (h->own_particles && h->particles) cudaFree(h->particles);
+    for (auto& s : h->scenes) {
+        if (s.col_data) cudaFree(s.col_data);
+        if (s.bvh) cudaFree(s.bvh);
+    }
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MPM_OK;
+}
+
+extern "C" const char* mpm_last_error(const MpmHandle* h) { return h ? h->err.c_str() : "null handle"; }
+
+extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
+    if (!cfg || !out) return MPM_ERR_ARG;
+    *out = nullptr;
+    MpmHandle* h = new MpmHandle();
+    h->cfg = *cfg;
+    h->device = cfg->device;
+    if (cfg->max_particles == 0) { *out = h; return fail(h, MPM_ERR_ARG, "max_particles must be > 0"); }
+    h->tile_edge = cfg->tile_edge ? cfg->tile_edge : 16u;
+    if (h->tile_edge != 8u && h->tile_edge != 16u) { *out = h; return fail(h, MPM_ERR_ARG, "tile_edge must be 8 or 16"); }
+    uint32_t max_scenes = cfg->max_scenes ? cfg->max_scenes : 1u;
+    if (max_scenes > 65534u) { *out = h; return fail(h, MPM_ERR_ARG, "max_scenes must be <= 65534"); }
+    uint32_t N = cfg->max_particles;
+    h->max_tiles = cfg->max_tiles ? cfg->max_tiles : std::max(1024u, std::min(N / 32u + 64u * max_scenes, 1u << 17));
+    uint32_t cap_req = cfg->hash_capacity ? cfg->hash_capacity : std::max(2u * h->max_tiles, 2u * std::min(N, 1u << 22));
+    h->cap = std::max(next_pow2(cap_req), (uint32_t)COMPACT_CHUNK);
+    *out = h;
+
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "cudaSetDevice(%d): %s", h->device, cudaGetErrorString(e));
+    CK(h, cudaDeviceGetAttribute(&h->n_sms, cudaDevAttrMultiProcessorCount, h->device));
+    if (cfg->stream) {
+        h->stream = (cudaStream_t)cfg->stream;
+    } else {
+        CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->own_stream = true;
+    }
+    size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
+    CK(h, cudaMalloc(&h->particles, (size_t)N * MPM_PARTICLE_BYTES));
+    CK(h, cudaMalloc(&h->order[0], (size_t)N * 4));
+    CK(h, cudaMalloc(&h->order[1], (size_t)N * 4));
+    CK(h, cudaMalloc(&h->bin_slot, (size_t)N * 4));
+    CK(h, cudaMalloc(&h->bin_rank, (size_t)N * 4));
+    CK(h, cudaMalloc(&h->keys, (size_t)h->cap * 8));
+    CK(h, cudaMalloc(&h->slot_count, (size_t)h->cap * 4));
+    CK(h, cudaMalloc(&h->slot_off, (size_t)h->cap * 4));
+    CK(h, cudaMalloc(&h->slot_st, (size_t)h->cap * 4));
+    CK(h, cudaMalloc(&h->st_key, (size_t)h->cap * 8));
+    CK(h, cudaMalloc(&h->st_slot, (size_t)h->cap * 4));
+    CK(h, cudaMalloc(&h->st_begin, (size_t)h->cap * 4));
+    CK(h, cudaMalloc(&h->st_count, (size_t)h->cap * 4));
+    CK(h, cudaMalloc(&h->chunk_nst, (size_t)(h->cap / COMPACT_CHUNK) * 4));
+    CK(h, cudaMalloc(&h->chunk_np, (size_t)(h->cap / COMPACT_CHUNK) * 4));
+    CK(h, cudaMalloc(&h->tiles[0], (size_t)h->max_tiles * NC * 16));
+    CK(h, cudaMalloc(&h->tiles[1], (size_t)h->max_tiles * NC * 16));
+    CK(h, cudaMalloc(&h->d_scenes, (size_t)max_scenes * sizeof(SceneDev)));
+    CK(h, cudaMalloc(&h->d_scene_first, (size_t)(max_scenes + 1) * 4));
+    CK(h, cudaMalloc(&h->counters, sizeof(Counters)));
+    CK(h, cudaMemsetAsync(h->keys, 0xff, (size_t)h->cap * 8, h->stream));
+    CK(h, cudaMemsetAsync(h->slot_count, 0, (size_t)h->cap * 4, h->stream));
+    CK(h, cudaMemsetAsync(h->counters, 0, sizeof(Counters), h->stream));
+    CK(h, cudaMemsetAsync(h->particles, 0, (size_t)N * MPM_PARTICLE_BYTES, h->stream));
+    h->scenes.resize(max_scenes);
+    for (auto& s : h->scenes) {
+        std::memset(s.uni, 0, sizeof(s.uni));
+        mpm_default_params(&s.params);
+        std::memset(&s.dev, 0, sizeof(s.dev));
+    }
+    h->n_scenes = 1;
+    h->scene_first.assign(2, 0);
+    h->n_particles = 0;
+    cudaError_t ce = (h->tile_edge == 8u) ? configure_tile_kernels<8>(h->blocks_per_sm)
+                                          : configure_tile_kernels<16>(h->blocks_per_sm);
+    if (ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "configure kernels: %s", cudaGetErrorString(ce));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+static int check_scene(MpmHandle* h, uint32_t scene) {
+    if (!h) return MPM_ERR_ARG;
+    if (scene >= h->scenes.size()) return fail(h, MPM_ERR_ARG, "scene %u out of range (max_scenes %zu)", scene, h->scenes.size());
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_uniforms(MpmHandle* h, uint32_t scene, const void* bytes, size_t n) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (!bytes || n < 544) return fail(h, MPM_ERR_ARG, "uniform block needs >= 544 bytes, got %zu", n);
+    SceneHost& s = h->scenes[scene];
+    uint8_t next[MPM_UNIFORMS_BYTES];
+    std::memset(next, 0, sizeof(next));
+    std::memcpy(next, bytes, std::min(n, (size_t)MPM_UNIFORMS_BYTES));
+    if (s.have_uniforms && std::memcmp(next, s.uni, sizeof(next)) == 0) return MPM_OK;
+    std::memcpy(s.uni, next, sizeof(next));
+    s.have_uniforms = true;
+    h->scenes_dirty = true;
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_params(MpmHandle* h, uint32_t scene, const MpmParams* p) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (!p) return fail(h, MPM_ERR_ARG, "null params");
+    if (p->n_iter == 0) return fail(h, MPM_ERR_ARG, "n_iter must be >= 1");
+    h->scenes[scene].params = *p;
+    h->scenes_dirty = true;
+    destroy_graphs(h);  // n_iter may have changed the schedule
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_scene_count(MpmHandle* h, uint32_t n_scenes) {
+    if (!h) return MPM_ERR_ARG;
+    if (n_scenes == 0 || n_scenes > h->scenes.size()) return fail(h, MPM_ERR_ARG, "bad scene count %u", n_scenes);
+    h->n_scenes = n_scenes;
+    h->scene_first.resize(n_scenes + 1, h->n_particles);
+    h->scenes_dirty = true;
+    destroy_graphs(h);
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_scene_range(MpmHandle* h, uint32_t scene, uint32_t first, uint32_t count) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (scene >= h->n_scenes) return fail(h, MPM_ERR_ARG, "scene %u >= scene count %u", scene, h->n_scenes);
+    h->scenes[scene].dev.p_first = first;
+    h->scenes[scene].dev.p_count = count;
+    h->scenes_dirty = true;
+    destroy_graphs(h);
+    return MPM_OK;
+}
+
+static int set_count(MpmHandle* h, uint32_t n) {
+    if (n != h->n_particles) {
+        h->n_particles = n;
+        h->order_valid = false;
+        destroy_graphs(h);
+        if (h->n_scenes == 1) {
+            h->scenes[0].dev.p_first = 0;
+            h->scenes[0].dev.p_count = n;
+            h->scenes_dirty = true;
+        }
+    }
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_particles(MpmHandle* h, const void* src, uint32_t n, int src_is_device) {
+    if (!h || (!src && n)) return MPM_ERR_ARG;
+    if (n > h->cfg.max_particles) return fail(h, MPM_ERR_CAPACITY, "%u particles > max_particles %u", n, h->cfg.max_particles);
+    if (!h->own_particles) return fail(h, MPM_ERR_STATE, "particles are bound to a caller buffer");
+    cudaSetDevice(h->device);
+    if (n) CK(h, cudaMemcpyAsync(h->particles, src, (size_t)n * MPM_PARTICLE_BYTES,
+                                 src_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+    set_count(h, n);
+    h->order_valid = false;
+    return MPM_OK;
+}
+
+extern "C" int mpm_get_particles(MpmHandle* h, void* dst, uint32_t n, int dst_is_device) {
+    if (!h || (!dst && n)) return MPM_ERR_ARG;
+    if (n > h->n_particles) return fail(h, MPM_ERR_ARG, "asked for %u particles, have %u", n, h->n_particles);
+    cudaSetDevice(h->device);
+    if (n) CK(h, cudaMemcpyAsync(dst, h->particles, (size_t)n * MPM_PARTICLE_BYTES,
+                                 dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    if (!dst_is_device) CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+extern "C" int mpm_bind_particles_device(MpmHandle* h, void* dptr, uint32_t n) {
+    if (!h || !dptr) return MPM_ERR_ARG;
+    if (n > h->cfg.max_particles) return fail(h, MPM_ERR_CAPACITY, "%u particles > max_particles %u", n, h->cfg.max_particles);
+    if (((uintptr_t)dptr & 15u) != 0) return fail(h, MPM_ERR_ARG, "particle buffer must be 16-byte aligned");
+    cudaSetDevice(h->device);
+    if (h->own_particles && h->particles) cudaFree(h->particles);
+    h->particles = (float4*)dptr;
+    h->own_particles = false;
+    destroy_graphs(h);
+    set_count(h, n);
+    h->order_valid = false;
+    return MPM_OK;
+}
+
+extern "C" void* mpm_particles_device_ptr(MpmHandle* h) { return h ? (void*)h->particles : nullptr; }
+
+extern "C" int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* data, size_t words, uint32_t num_indices,
+                                const void* nodes, uint32_t n_nodes) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if ((words && !data) || (n_nodes && !nodes)) return fail(h, MPM_ERR_ARG, "null collider buffer");
+    if ((size_t)num_indices > words) return fail(h, MPM_ERR_ARG, "num_indices %u > words %zu", num_indices, words);
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    SceneHost& s = h->scenes[scene];
+    if (s.col_data) { cudaFree(s.col_data); s.col_data = nullptr; }
+    if (s.bvh) { cudaFree(s.bvh); s.bvh = nullptr; }
+    if (words) {
+        CK(h, cudaMalloc(&s.col_data, words * 4));
+        CK(h, cudaMemcpy(s.col_data, data, words * 4, cudaMemcpyHostToDevice));
+    }
+    if (n_nodes) {
+        CK(h, cudaMalloc(&s.bvh, (size_t)n_nodes * MPM_BVH_NODE_BYTES));
+        CK(h, cudaMemcpy(s.bvh, nodes, (size_t)n_nodes * MPM_BVH_NODE_BYTES, cudaMemcpyHostToDevice));
+    }
+    s.dev.col_data = s.col_data;
+    s.dev.bvh = s.bvh;
+    s.dev.col_words = (uint32_t)words;
+    s.dev.n_nodes = n_nodes;
+    s.dev.c_nidx = num_indices;  // GpuMpmPipelineManager.ts:80 writes colliderNumIndices
+    if (s.have_uniforms) std::memcpy(s.uni + 348, &num_indices, 4);
+    h->scenes_dirty = true;
+    return MPM_OK;
+}
+
+static int upload_scenes(MpmHandle* h) {
+    if (!h->scenes_dirty) return MPM_OK;
+    // scene ranges must tile [0, n_particles)
+    std::vector<uint32_t> first(h->n_scenes + 1);
+    uint32_t expect = 0;
+    for (uint32_t s = 0; s < h->n_scenes; s++) {
+        SceneHost& sc = h->scenes[s];
+        if (!sc.have_uniforms) return fail(h, MPM_ERR_STATE, "scene %u has no uniforms", s);
+        if (sc.dev.p_first != expect)
+            return fail(h, MPM_ERR_ARG, "scene %u starts at %u, expected %u (ranges must tile the buffer)", s, sc.dev.p_first, expect);
+        first[s] = expect;
+        expect += sc.dev.p_count;
+        build_scene_dev(sc);
+        if (sc.dev.scale <= 0.0f || !(sc.dev.dt > 0.0f))
+            return fail(h, MPM_ERR_ARG, "scene %u: fixedPointScale and timestep must be > 0", s);
+        if (sc.dev.res[0] <= 0 || sc.dev.res[1] <= 0 || sc.dev.res[2] <= 0)
+            return fail(h, MPM_ERR_ARG, "scene %u: grid resolution must be > 0", s);
+        if (sc.params.n_iter != h->scenes[0].params.n_iter)
+            return fail(h, MPM_ERR_ARG, "all scenes of a handle must share n_iter");
+    }
+    if (expect != h->n_particles)
+        return fail(h, MPM_ERR_ARG, "scene ranges cover %u particles, buffer holds %u", expect, h->n_particles);
+    first[h->n_scenes] = expect;
+    h->scene_first = first;
+    std::vector<SceneDev> tmp(h->n_scenes);
+    for (uint32_t s = 0; s < h->n_scenes; s++) tmp[s] = h->scenes[s].dev;
+    CK(h, cudaMemcpyAsync(h->d_scenes, tmp.data(), tmp.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->d_scene_first, h->scene_first.data(), h->scene_first.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));  // host staging vectors go out of scope
+    h->scenes_dirty = false;
+    return MPM_OK;
+}
+
+// identity order for the first substep after new particles
+__global__ void k_iota(uint32_t* o, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = i;
+}
+
+static Ctx make_ctx(MpmHandle* h, int parity) {
+    Ctx c{};
+    c.particles = h->particles;
+    c.order_in = h->order[parity];
+    c.sorted = h->order[parity ^ 1];
+    c.bin_slot = h->bin_slot;
+    c.bin_rank = h->bin_rank;
+    c.keys = h->keys;
+    c.slot_count = h->slot_count;
+    c.slot_off = h->slot_off;
+    c.slot_st = h->slot_st;
+    c.st_key = h->st_key;
+    c.st_slot = h->st_slot;
+    c.st_begin = h->st_begin;
+    c.st_count = h->st_count;
+    c.chunk_nst = h->chunk_nst;
+    c.chunk_np = h->chunk_np;
+    c.tiles_a = h->tiles[0];
+    c.tiles_b = h->tiles[0];
+    c.scenes = h->d_scenes;
+    c.scene_first = h->d_scene_first;
+    c.counters = h->counters;
+    c.n_particles = h->n_particles;
+    c.n_scenes = h->n_scenes;
+    c.cap = h->cap;
+    c.max_tiles = h->max_tiles;
+    return c;
+}
+
+static cudaEvent_t get_event(MpmHandle* h) {
+    if (!h->event_pool.empty()) {
+        cudaEvent_t e = h->event_pool.back();
+        h->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+static void drain_timing(MpmHandle* h) {
+    if (h->pending.empty()) return;
+    cudaStreamSynchronize(h->stream);
+    for (auto& t : h->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+            h->kms[t.kid] += ms;
+            h->kcount[t.kid] += 1;
+        }
+        h->event_pool.push_back(t.a);
+        h->event_pool.push_back(t.b);
+    }
+    h->pending.clear();
+}
+
+static cudaError_t launch(MpmHandle* h, uint32_t kid, const Ctx& c, bool capturing) {
+    int grid = std::max(1, h->n_sms * std::max(1, h->blocks_per_sm[kid]));
+    bool timed = h->timing && !capturing;
+    TimedLaunch tl{kid, nullptr, nullptr};
+    if (timed) {
+        tl.a = get_event(h);
+        tl.b = get_event(h);
+        cudaEventRecord(tl.a, h->stream);
+    }
+    cudaError_t e = (h->tile_edge == 8u) ? launch_kernel<8>(kid, c, h->stream, grid, 0, 0, nullptr)
+                                         : launch_kernel<16>(kid, c, h->stream, grid, 0, 0, nullptr);
+    if (timed) {
+        cudaEventRecord(tl.b, h->stream);
+        h->pending.push_back(tl);
+        if (h->pending.size() > 4096) drain_timing(h);
+    }
+    return e;
+}
+
+// One substep's launch sequence (GpuMpmPipelineManager.ts:327-428 explicit,
+// :431-521 PBMPM).  stop_p2g ends after the first particle-to-grid pass.
+static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool capturing, bool stop_p2g) {
+    Ctx c = make_ctx(h, parity);
+    cudaError_t e;
+#define L(k)                                   \
+    do {                                       \
+        e = launch(h, (k), c, capturing);      \
+        if (e != cudaSuccess) return e;        \
+    } while (0)
+    L(K_CLEAR_TABLE);
+    L(K_BIN_INSERT);
+    L(K_COMPACT_A);
+    L(K_COMPACT_B);
+    L(K_COMPACT_C);
+    L(K_BIN_SCATTER);
+    if (method == MPM_METHOD_EXPLICIT) {
+        c.tiles_a = h->tiles[0];
+        L(K_P2G_EXPLICIT);
+        if (stop_p2g) { h->last_tiles = 0; return cudaSuccess; }
+        c.tiles_b = h->tiles[0];
+        L(K_G2P_EXPLICIT);
+        h->last_tiles = 0;
+    } else {
+        uint32_t n_iter = h->scenes[0].params.n_iter;
+        int cur = 0;
+        c.tiles_a = h->tiles[cur];
+        L(K_PBMPM_FIRST);
+        if (stop_p2g) { h->last_tiles = cur; return cudaSuccess; }
+        for (uint32_t it = 1; it < n_iter; it++) {
+            c.tiles_b = h->tiles[cur];
+            c.tiles_a = h->tiles[cur ^ 1];
+            L(K_PBMPM_ITER);
+            cur ^= 1;
+        }
+        c.tiles_b = h->tiles[cur];
+        L(K_G2P_PBMPM);
+        h->last_tiles = cur;
+    }
+#undef L
+    return cudaSuccess;
+}
+
+static int prepare_step(MpmHandle* h) {
+    if (h->n_particles == 0) return fail(h, MPM_ERR_STATE, "no particles");
+    cudaSetDevice(h->device);
+    int r = upload_scenes(h);
+    if (r) return r;
+    if (!h->order_valid) {
+        // both order buffers start as the identity so every entry the next
+        // binning pass reads is a valid particle index
+        k_iota<<<(h->n_particles + 255) / 256, 256, 0, h->stream>>>(h->order[0], h->n_particles);
+        CK(h, cudaGetLastError());
+        k_iota<<<(h->n_particles + 255) / 256, 256, 0, h->stream>>>(h->order[1], h->n_particles);
+        CK(h, cudaGetLastError());
+        h->order_valid = true;
+    }
+    return MPM_OK;
+}
+
+static uint64_t graph_signature(MpmHandle* h) {
+    uint64_t s = h->n_particles;
+    s = s * 1315423911ull + h->n_scenes;
+    s = s * 1315423911ull + h->scenes[0].params.n_iter;
+    s = s * 1315423911ull + (uint64_t)(uintptr_t)h->particles;
+    return s | 1ull;
+}
+
+static int run_substep(MpmHandle* h, int method) {
+    int par = h->order_parity;
+    if (h->use_graphs && !h->timing) {
+        uint64_t sig = graph_signature(h);
+        if (!h->graph[method][par] || h->graph_sig[method][par] != sig) {
+            if (h->graph[method][par]) cudaGraphExecDestroy(h->graph[method][par]);
+            h->graph[method][par] = nullptr;
+            cudaGraph_t g;
+            CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = enqueue_substep(h, method, par, true, false);
+            cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+            if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
+            if (e2 != cudaSuccess) return fail(h, MPM_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
+            cudaError_t e3 = cudaGraphInstantiate(&h->graph[method][par], g, 0);
+            cudaGraphDestroy(g);
+            if (e3 != cudaSuccess) return fail(h, MPM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e3));
+            h->graph_sig[method][par] = sig;
+        }
+        CK(h, cudaGraphLaunch(h->graph[method][par], h->stream));
+        // the captured sequence leaves its last P2G result in the same buffer
+        h->last_tiles = (method == MPM_METHOD_EXPLICIT) ? 0 : (int)((h->scenes[0].params.n_iter - 1) & 1u);
+    } else {
+        cudaError_t e = enqueue_substep(h, method, par, false, false);
+        if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    }
+    h->order_parity ^= 1;
+    return MPM_OK;
+}
+
+extern "C" int mpm_step(MpmHandle* h, int method, uint32_t n_substeps) {
+    if (!h) return MPM_ERR_ARG;
+    if (method != MPM_METHOD_EXPLICIT && method != MPM_METHOD_PBMPM) return fail(h, MPM_ERR_ARG, "bad method %d", method);
+    int r = prepare_step(h);
+    if (r) return r;
+    for (uint32_t i = 0; i < n_substeps; i++) {
+        r = run_substep(h, method);
+        if (r) return r;
+    }
+    return MPM_OK;
+}
+
+extern "C" int mpm_add_explicit_mpm_dispatches(MpmHandle* h, uint32_t n_particles) {
+    if (!h) return MPM_ERR_ARG;
+    if (n_particles != h->n_particles) return fail(h, MPM_ERR_ARG, "nParticles %u != bound %u", n_particles, h->n_particles);
+    return mpm_step(h, MPM_METHOD_EXPLICIT, 1);
+}
+
+extern "C" int mpm_add_pbmpm_dispatches(MpmHandle* h, uint32_t n_particles) {
+    if (!h) return MPM_ERR_ARG;
+    if (n_particles != h->n_particles) return fail(h, MPM_ERR_ARG, "nParticles %u != bound %u", n_particles, h->n_particles);
+    return mpm_step(h, MPM_METHOD_PBMPM, 1);
+}
+
+extern "C" int mpm_step_p2g_only(MpmHandle* h, int method) {
+    if (!h) return MPM_ERR_ARG;
+    if (method != MPM_METHOD_EXPLICIT && method != MPM_METHOD_PBMPM) return fail(h, MPM_ERR_ARG, "bad method %d", method);
+    int r = prepare_step(h);
+    if (r) return r;
+    cudaError_t e = enqueue_substep(h, method, h->order_parity, false, true);
+    if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    h->order_parity ^= 1;
+    return MPM_OK;
+}
+
+extern "C" int mpm_sync(MpmHandle* h, uint32_t* status_out) {
+    if (!h) return MPM_ERR_ARG;
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    Counters ct;
+    CK(h, cudaMemcpy(&ct, h->counters, sizeof(ct), cudaMemcpyDeviceToHost));
+    if (status_out) *status_out = ct.status;
+    if (ct.status) return fail(h, MPM_ERR_DEVICE_STATUS, "device status 0x%x", ct.status);
+    return MPM_OK;
+}
+
+extern "C" int mpm_clear_status(MpmHandle* h) {
+    if (!h) return MPM_ERR_ARG;
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    uint32_t z = 0;
+    CK(h, cudaMemcpy(&h->counters->status, &z, 4, cudaMemcpyHostToDevice));
+    return MPM_OK;
+}
+
+extern "C" int mpm_get_counts(MpmHandle* h, uint32_t* n_tiles, uint32_t* n_binned) {
+    if (!h) return MPM_ERR_ARG;
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    Counters ct;
+    CK(h, cudaMemcpy(&ct, h->counters, sizeof(ct), cudaMemcpyDeviceToHost));
+    if (n_tiles) *n_tiles = ct.n_st;
+    if (n_binned) *n_binned = ct.n_binned;
+    return MPM_OK;
+}
+
+extern "C" int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_update, int32_t* out_host, size_t n_cells) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (scene >= h->n_scenes) return fail(h, MPM_ERR_ARG, "scene %u >= scene count", scene);
+    const SceneDev& d = h->scenes[scene].dev;
+    size_t need = (size_t)d.res[0] * d.res[1] * d.res[2];
+    if (!out_host || n_cells < need) return fail(h, MPM_ERR_ARG, "grid buffer needs %zu cells", need);
+    cudaSetDevice(h->device);
+    int4* dout = nullptr;
+    CK(h, cudaMalloc(&dout, need * 16));
+    CK(h, cudaMemsetAsync(dout, 0, need * 16, h->stream));
+    Ctx c = make_ctx(h, h->order_parity);
+    c.tiles_b = h->tiles[h->last_tiles];
+    int grid = std::max(1, h->n_sms * std::max(1, h->blocks_per_sm[K_GRID_DENSE]));
+    cudaError_t e = (h->tile_edge == 8u) ? launch_kernel<8>(K_GRID_DENSE, c, h->stream, grid, scene, apply_grid_update, dout)
+                                         : launch_kernel<16>(K_GRID_DENSE, c, h->stream, grid, scene, apply_grid_update, dout);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_host, dout, need * 16, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "grid readback: %s", cudaGetErrorString(e));
+    return MPM_OK;
+}
+
+extern "C" int mpm_enable_kernel_timing(MpmHandle* h, int enable) {
+    if (!h) return MPM_ERR_ARG;
+    drain_timing(h);
+    h->timing = enable != 0;
+    for (int k = 0; k < K_COUNT; k++) { h->kms[k] = 0; h->kcount[k] = 0; }
+    return MPM_OK;
+}
+
+extern "C" int mpm_kernel_times(MpmHandle* h, float* ms_out, uint32_t* launches_out, uint32_t n_kernels) {
+    if (!h) return MPM_ERR_ARG;
+    drain_timing(h);
+    for (uint32_t k = 0; k < n_kernels && k < (uint32_t)K_COUNT; k++) {
+        if (ms_out) ms_out[k] = (float)h->kms[k];
+        if (launches_out) launches_out[k] = h->kcount[k];
+    }
+    return MPM_OK;
+}
+
+extern "C" const char* mpm_kernel_name(uint32_t kernel_id) {
+    return kernel_id < (uint32_t)K_COUNT ? kKernelNames[kernel_id] : "unknown";
+}
+
+extern "C" uint32_t mpm_kernel_count(void) { return (uint32_t)K_COUNT; }
+
+extern "C" int mpm_use_graphs(MpmHandle* h, int enable) {
+    if (!h) return MPM_ERR_ARG;
+    h->use_graphs = enable != 0;
+    if (!h->use_graphs) destroy_graphs(h);
+    return MPM_OK;
+}

@@ -1,0 +1,132 @@
+// mpm_engine.cuh -- device-side data layout of the MPM step.
+//
+// HBM layout (all buffers allocated once by mpm_create):
+//   particles   N x 192 B  reference ParticleData records, never reordered
+//   order[2]    N x u32    particle ids in the previous substep's tile order
+//   bin_slot    N x u32    tile hash slot of the particle at order position t
+//   bin_rank    N x u32    its rank inside that tile
+//   sorted      = order[next]: particle ids grouped by tile
+//   keys        cap x u64  open-addressing tile hash (hash3 of the tile coord,
+//                          linear probing); EMPTY = ~0
+//   slot_count  cap x u32  particles per slot
+//   slot_off, slot_st      per-slot particle offset and compact tile index
+//   st_key/st_slot/st_begin/st_count   per compact tile
+//   tiles[2]    max_tiles x (E+2)^3 x int4   per-tile halo sums
+//               (mass, momentum x, y, z) in the reference i32 fixed point
+//
+// A tile is E^3 grid cells (E = 8 or 16, i.e. 2^3 or 4^3 of the reference's
+// 4^3-cell blocks).  Its P2G writes the (E+2)^3 halo region it touches; the
+// grid value of a cell is the i32 sum over every tile halo that covers it
+// (at most 8), formed on the fly by the G2P kernels.  Integer addition
+// commutes, so the sums equal the reference's atomicAdd totals exactly.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpm {
+
+constexpr uint64_t KEY_EMPTY = ~0ull;
+constexpr uint32_t INVALID = 0xFFFFFFFFu;
+constexpr uint32_t MAX_PROBES = 1024u;
+constexpr int COMPACT_CHUNK = 4096;   // hash slots per compaction block (256 threads x 16)
+constexpr int KEY_BIAS = 32768;
+
+// status bits (mirror of MPM_STATUS_* in include/mpm.h)
+constexpr uint32_t ST_HASH_FULL = 0x1u;
+constexpr uint32_t ST_TILE_OVERFLOW = 0x2u;
+constexpr uint32_t ST_BVH_STACK = 0x4u;
+constexpr uint32_t ST_SCENE_RANGE = 0x8u;
+constexpr uint32_t ST_MLP_FALLBACK = 0x10u;
+
+// Per-scene parameters: the uniform fields the step reads plus the
+// extension constants, laid out for a word-wise copy into shared memory.
+struct SceneDev {
+    float dt, scale;
+    float gmin[3], gmax[3], cd[3];
+    int32_t res[3];
+    float cmin[3], cmax[3];
+    float xf[16], xfi[16];
+    float cvel[3];
+    uint32_t c_nidx, c_nobj;
+    float ipos[3], istr, irad;
+    uint32_t iact, imode;
+    float g[3], mu0, la0, xi_e, xi_p, smin, smax, inv_rho;
+    uint32_t n_iter;
+    float fdiv;
+    uint32_t bmode;
+    float rest;
+    int32_t bc;
+    uint32_t gaxis;
+    float cmargin, csurf, cthr, cfric, cvs, blend, vexp;
+    uint32_t p_first, p_count;
+    uint32_t col_words, n_nodes;
+    const uint32_t* col_data;
+    const uint32_t* bvh;
+    uint32_t scale_is_pow2;
+    float inv_scale;
+    uint32_t pad[2];
+};
+static_assert(sizeof(SceneDev) % 8 == 0, "SceneDev must be 8-byte sized");
+
+struct Counters {
+    uint32_t n_st;       // occupied tiles of the current substep
+    uint32_t n_binned;   // particles placed in tiles
+    uint32_t status;     // sticky status bits
+    uint32_t pad;
+};
+
+struct Ctx {
+    float4* particles;        // N x 12 float4
+    const uint32_t* order_in; // previous tile order
+    uint32_t* sorted;         // this substep's tile order
+    uint32_t* bin_slot;
+    uint32_t* bin_rank;
+    unsigned long long* keys;
+    uint32_t* slot_count;
+    uint32_t* slot_off;
+    uint32_t* slot_st;
+    unsigned long long* st_key;
+    uint32_t* st_slot;
+    uint32_t* st_begin;
+    uint32_t* st_count;
+    uint32_t* chunk_nst;
+    uint32_t* chunk_np;
+    int4* tiles_a;            // tiles written by this pass's P2G
+    int4* tiles_b;            // tiles read by this pass's G2P
+    const SceneDev* scenes;
+    const uint32_t* scene_first;  // n_scenes + 1 particle offsets
+    Counters* counters;
+    uint32_t n_particles;
+    uint32_t n_scenes;
+    uint32_t cap;             // hash capacity, power of two
+    uint32_t max_tiles;
+};
+
+__host__ __device__ inline uint64_t pack_key(uint32_t scene, int sx, int sy, int sz) {
+    return ((uint64_t)scene << 48) | ((uint64_t)(uint32_t)(sx + KEY_BIAS) << 32) |
+           ((uint64_t)(uint32_t)(sy + KEY_BIAS) << 16) | (uint64_t)(uint32_t)(sz + KEY_BIAS);
+}
+__host__ __device__ inline void unpack_key(uint64_t k, uint32_t& scene, int& sx, int& sy, int& sz) {
+    scene = (uint32_t)(k >> 48);
+    sx = (int)((k >> 32) & 0xffff) - KEY_BIAS;
+    sy = (int)((k >> 16) & 0xffff) - KEY_BIAS;
+    sz = (int)(k & 0xffff) - KEY_BIAS;
+}
+
+enum KernelId : uint32_t {
+    K_CLEAR_TABLE = 0,
+    K_BIN_INSERT,
+    K_COMPACT_A,
+    K_COMPACT_B,
+    K_COMPACT_C,
+    K_BIN_SCATTER,
+    K_P2G_EXPLICIT,
+    K_G2P_EXPLICIT,
+    K_PBMPM_FIRST,
+    K_PBMPM_ITER,
+    K_G2P_PBMPM,
+    K_GRID_DENSE,
+    K_COUNT
+};
+
+}  // namespace mpm

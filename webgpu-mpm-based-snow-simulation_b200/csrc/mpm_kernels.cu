@@ -1,0 +1,1231 @@
+// mpm_kernels.cu -- the MPM substep as CUDA kernels for sm_100a.
+//
+// Substep (explicit):  clear_table -> bin_insert -> compact_{a,b,c} -> bin_scatter
+//                      -> p2g_explicit -> g2p_explicit (G2P + integrate fused)
+// Substep (PBMPM, n_iter iterations):  same binning, then
+//                      pbmpm_first (constraints + affine P2G + forces)
+//                      -> (n_iter-1) x pbmpm_iter (G2P, constraints, P2G fused)
+//                      -> g2p_pbmpm (last G2P + integrate fused)
+//
+// The reference runs the same math as 11 (explicit) or 16 (PBMPM, 3 iters)
+// WGSL dispatches (src/lib/gpu/mpm/GpuMpmPipelineManager.ts:327-521) with
+// 108 global i32 atomics per particle per transfer; here each tile's
+// particles accumulate into a shared-memory halo tile and the tile is
+// written once with plain 16-byte stores.
+#include "mpm_engine.cuh"
+#include "mpm_math.cuh"
+
+namespace mpm {
+
+// ------------------------------------------------------------------
+// shared helpers
+// ------------------------------------------------------------------
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t tile_hash(uint32_t scene, int sx, int sy, int sz) {
+    return hash3((uint32_t)sx, (uint32_t)sy, (uint32_t)sz) ^ (scene * 0x9E3779B1u);
+}
+
+__device__ uint32_t tile_insert(const Ctx& c, uint64_t key, uint32_t scene, int sx, int sy, int sz) {
+    uint32_t mask = c.cap - 1u;
+    uint32_t s = tile_hash(scene, sx, sy, sz) & mask;
+    uint32_t limit = c.cap < MAX_PROBES ? c.cap : MAX_PROBES;
+    for (uint32_t probe = 0; probe < limit; probe++) {
+        unsigned long long k = *((volatile unsigned long long*)&c.keys[s]);
+        if (k == key) return s;
+        if (k == KEY_EMPTY) {
+            unsigned long long old = atomicCAS(&c.keys[s], KEY_EMPTY, (unsigned long long)key);
+            if (old == KEY_EMPTY || old == key) return s;
+        }
+        s = (s + 1u) & mask;
+    }
+    atomicOr(&c.counters->status, ST_HASH_FULL);
+    return INVALID;
+}
+
+__device__ uint32_t tile_lookup(const Ctx& c, uint64_t key, uint32_t scene, int sx, int sy, int sz) {
+    uint32_t mask = c.cap - 1u;
+    uint32_t s = tile_hash(scene, sx, sy, sz) & mask;
+    uint32_t limit = c.cap < MAX_PROBES ? c.cap : MAX_PROBES;
+    for (uint32_t probe = 0; probe < limit; probe++) {
+        unsigned long long k = c.keys[s];
+        if (k == key) return s;
+        if (k == KEY_EMPTY) return INVALID;
+        s = (s + 1u) & mask;
+    }
+    return INVALID;
+}
+
+__device__ __forceinline__ uint32_t find_scene(const Ctx& c, uint32_t p) {
+    uint32_t lo = 0, hi = c.n_scenes;  // answer in [0, n_scenes)
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&c.scene_first[mid]) <= p) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <int E>
+struct TileGeom {
+    static constexpr int H = E + 2;
+    static constexpr int NC = H * H * H;
+    static constexpr int SHIFT = (E == 8) ? 3 : 4;
+};
+
+__device__ __forceinline__ void load_scene_smem(SceneDev& dst, const SceneDev* src) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(SceneDev) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+__device__ __forceinline__ float inv_s(const SceneDev& S, int32_t v) {
+    // f32(i) / fixedPointScale; multiplication by the exact reciprocal when
+    // the scale is a power of two gives the identical f32 result.
+    return S.scale_is_pow2 ? fm(i2f(v), S.inv_scale) : fd(i2f(v), S.scale);
+}
+
+// Grid-side boundary of boundary_mode 1 (an extension; the reference only
+// reflects particles): sticky ground plane, slip walls.
+__device__ __forceinline__ void grid_bc(const SceneDev& S, const int* gc, float* v) {
+    if (S.bmode != 1u) return;
+    if (gc[S.gaxis] < S.bc) { v[0] = 0.f; v[1] = 0.f; v[2] = 0.f; return; }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (gc[a] < S.bc && v[a] < 0.f) v[a] = 0.f;
+        if (gc[a] >= S.res[a] - S.bc && v[a] > 0.f) v[a] = 0.f;
+    }
+}
+
+// ------------------------------------------------------------------
+// particle record access (192 B = 12 float4)
+// ------------------------------------------------------------------
+struct PState {
+    float pos[3], hom, vel[3], mass;
+    float Fe[9], Fp[9], dxp[3], D[9];
+};
+
+__device__ __forceinline__ void unpack_m(const float4& a, const float4& b, const float4& c, float* m) {
+    m[0] = a.x; m[1] = a.y; m[2] = a.z;
+    m[3] = b.x; m[4] = b.y; m[5] = b.z;
+    m[6] = c.x; m[7] = c.y; m[8] = c.z;
+}
+
+template <bool RO>
+__device__ __forceinline__ float4 ld4(const float4* p) {
+    if (RO) return __ldg(p);
+    return *p;
+}
+
+// loads record words [0, nq) float4s
+template <bool RO>
+__device__ __forceinline__ void load_particle(const float4* rec, PState& s, bool want_vel, bool want_dx_d) {
+    float4 q0 = ld4<RO>(rec + 0), q1 = ld4<RO>(rec + 1);
+    s.pos[0] = q0.x; s.pos[1] = q0.y; s.pos[2] = q0.z; s.hom = q0.w;
+    s.vel[0] = q1.x; s.vel[1] = q1.y; s.vel[2] = q1.z; s.mass = q1.w;
+    (void)want_vel;
+    unpack_m(ld4<RO>(rec + 2), ld4<RO>(rec + 3), ld4<RO>(rec + 4), s.Fe);
+    unpack_m(ld4<RO>(rec + 5), ld4<RO>(rec + 6), ld4<RO>(rec + 7), s.Fp);
+    if (want_dx_d) {
+        float4 q8 = ld4<RO>(rec + 8);
+        s.dxp[0] = q8.x; s.dxp[1] = q8.y; s.dxp[2] = q8.z;
+        unpack_m(ld4<RO>(rec + 9), ld4<RO>(rec + 10), ld4<RO>(rec + 11), s.D);
+    }
+}
+
+__device__ __forceinline__ void store_particle(float4* rec, const PState& s) {
+    rec[0] = make_float4(s.pos[0], s.pos[1], s.pos[2], s.hom);
+    rec[1] = make_float4(s.vel[0], s.vel[1], s.vel[2], s.mass);
+    rec[2] = make_float4(s.Fe[0], s.Fe[1], s.Fe[2], 0.f);
+    rec[3] = make_float4(s.Fe[3], s.Fe[4], s.Fe[5], 0.f);
+    rec[4] = make_float4(s.Fe[6], s.Fe[7], s.Fe[8], 0.f);
+    rec[5] = make_float4(s.Fp[0], s.Fp[1], s.Fp[2], 0.f);
+    rec[6] = make_float4(s.Fp[3], s.Fp[4], s.Fp[5], 0.f);
+    rec[7] = make_float4(s.Fp[6], s.Fp[7], s.Fp[8], 0.f);
+    rec[8] = make_float4(s.dxp[0], s.dxp[1], s.dxp[2], 0.f);
+    rec[9] = make_float4(s.D[0], s.D[1], s.D[2], 0.f);
+    rec[10] = make_float4(s.D[3], s.D[4], s.D[5], 0.f);
+    rec[11] = make_float4(s.D[6], s.D[7], s.D[8], 0.f);
+}
+
+// cell number, fractional position, quadratic B-spline weights
+// (mpmOps.wgsl:14-53)
+struct Stencil {
+    int cell[3];
+    float f[3];
+    float w[3][3];   // w[k][axis], k = offset + 1
+};
+
+__device__ __forceinline__ void make_stencil(const SceneDev& S, const float* pos, Stencil& st) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) st.cell[i] = f2i(fd(fs(pos[i], S.gmin[i]), S.cd[i]));
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        float mn = fa(S.gmin[i], fm(S.cd[i], i2f(st.cell[i])));
+        float f = fd(fs(pos[i], mn), S.cd[i]);
+        st.f[i] = f;
+        float om = fs(1.0f, f);
+        st.w[0][i] = fm(fm(0.5f, om), om);
+        float h = fs(f, 0.5f);
+        st.w[1][i] = fs(0.75f, fm(h, h));
+        st.w[2][i] = fm(fm(0.5f, f), f);
+    }
+}
+
+__device__ __forceinline__ float dwk(int k, float f) {
+    // derivative of the B-spline weights wrt the fractional position
+    return k == 0 ? fs(f, 1.0f) : (k == 1 ? fm(-2.0f, fs(f, 0.5f)) : f);
+}
+
+// ------------------------------------------------------------------
+// constitutive pieces
+// ------------------------------------------------------------------
+// hardenLameParameters + calculateStressFirstPiolaKirchhoff
+// (stressTensorOps.wgsl:9-22, 39-56); returns M = (-V) * P^T.
+__device__ __forceinline__ void stress_matrix(const SceneDev& S, const PState& p, float* M) {
+    float Jp = det3(p.Fp);
+    float ef = expf_m(fm(S.xi_e, fs(1.0f, Jp)));
+    float mu = fm(S.mu0, ef);
+    float la = fm(S.la0, ef);
+    float J = det3(p.Fe);
+    float R[9], Fi[9];
+    polar3(p.Fe, R);
+    inv3(p.Fe, Fi);
+    float a = fm(2.0f, mu);
+    float b = fm(fm(la, fs(J, 1.0f)), J);
+    float V = fm(p.mass, S.inv_rho);
+    float nV = -V;
+    // P[c][r] = a*(F[c][r]-R[c][r]) + b*Fi^T[c][r], Fi^T[c][r] = Fi[r][c]
+    // M[c][r] = (-V) * P^T[c][r] = (-V) * P[r][c]
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            float Prc = fa(fm(a, fs(p.Fe[r * 3 + c], R[r * 3 + c])), fm(b, Fi[c * 3 + r]));
+            M[c * 3 + r] = fm(nV, Prc);
+        }
+}
+
+// solveParticleConstraints (pbmpm.wgsl:16-39): updates D.
+__device__ __forceinline__ void pbmpm_constraints(const SceneDev& S, const float* Fe, const float* Fp, float* D) {
+    float IpD[9], Ft[9], Rt[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) IpD[i] = fa((i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f, D[i]);
+    mul3(IpD, Fe, Ft);
+    polar3(Ft, Rt);
+    float tv = det3(Ft);
+    float vs = powf_m(fabsf(tv), S.vexp);
+    float ob = fs(1.0f, S.blend);
+    float tb[9], Fei[9], Dc[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) tb[i] = fa(fm(S.blend, fm(Rt[i], vs)), fm(ob, Rt[i]));
+    inv3(Fe, Fei);
+    mul3(tb, Fei, Dc);
+    float J = det3(Fp);
+    float relax = fa(0.5f, fm(0.5f, fs(1.0f, expf_m(fd(-S.xi_p, J)))));
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        float dci = fs(Dc[i], (i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f);
+        D[i] = fa(D[i], fm(relax, fs(dci, D[i])));
+    }
+}
+
+// applyPlasticity (plasticityOps.wgsl:7-48)
+__device__ __forceinline__ void plasticity(const SceneDev& S, float* Fe, float* Fp) {
+    float R[9], Rt[9], Sm[9];
+    polar3(Fe, R);
+    tr3(R, Rt);
+    mul3(Rt, Fe, Sm);
+    float sg0 = Sm[0], sg1 = Sm[4], sg2 = Sm[8];
+    if (S.smin <= sg0 && S.smin <= sg1 && S.smin <= sg2 && sg0 <= S.smax && sg1 <= S.smax && sg2 <= S.smax) return;
+    float c0 = fminf(fmaxf(sg0, S.smin), S.smax);
+    float c1 = fminf(fmaxf(sg1, S.smin), S.smax);
+    float c2 = fminf(fmaxf(sg2, S.smin), S.smax);
+    float Dg[9] = {c0, 0.f, 0.f, 0.f, c1, 0.f, 0.f, 0.f, c2};
+    float Fn[9], Fni[9], F[9];
+    mul3(R, Dg, Fn);
+    inv3(Fn, Fni);
+    mul3(Fe, Fp, F);
+    mul3(Fni, F, Fp);
+#pragma unroll
+    for (int i = 0; i < 9; i++) Fe[i] = Fn[i];
+}
+
+// ------------------------------------------------------------------
+// collider (colliderPrelude.wgsl:29-356)
+// ------------------------------------------------------------------
+__device__ __forceinline__ void col_vertex(const SceneDev& S, uint32_t idx, float* v) {
+    uint32_t base = S.c_nidx + idx * 3u;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        uint32_t w = (base + (uint32_t)k < S.col_words) ? __ldg(&S.col_data[base + k]) : 0u;
+        v[k] = __uint_as_float(w);
+    }
+}
+
+__device__ void closest_point_tri(const float* p, const float* a, const float* b, const float* c, float* o) {
+    float ab[3], ac[3], ap[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) { ab[k] = fs(b[k], a[k]); ac[k] = fs(c[k], a[k]); ap[k] = fs(p[k], a[k]); }
+    float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+    if (d1 <= 0.f && d2 <= 0.f) { o[0] = a[0]; o[1] = a[1]; o[2] = a[2]; return; }
+    float bp[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) bp[k] = fs(p[k], b[k]);
+    float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 >= 0.f && d4 <= d3) { o[0] = b[0]; o[1] = b[1]; o[2] = b[2]; return; }
+    float vc = fs(fm(d1, d4), fm(d3, d2));
+    if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+        float v = fd(d1, fs(d1, d3));
+#pragma unroll
+        for (int k = 0; k < 3; k++) o[k] = fa(a[k], fm(v, ab[k]));
+        return;
+    }
+    float cp[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) cp[k] = fs(p[k], c[k]);
+    float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+    if (d6 >= 0.f && d5 <= d6) { o[0] = c[0]; o[1] = c[1]; o[2] = c[2]; return; }
+    float vb = fs(fm(d5, d2), fm(d1, d6));
+    if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+        float w = fd(d2, fs(d2, d6));
+#pragma unroll
+        for (int k = 0; k < 3; k++) o[k] = fa(a[k], fm(w, ac[k]));
+        return;
+    }
+    float va = fs(fm(d3, d6), fm(d5, d4));
+    if (va <= 0.f && fs(d4, d3) >= 0.f && fs(d5, d6) >= 0.f) {
+        float w = fd(fs(d4, d3), fa(fs(d4, d3), fs(d5, d6)));
+#pragma unroll
+        for (int k = 0; k < 3; k++) o[k] = fa(b[k], fm(w, fs(c[k], b[k])));
+        return;
+    }
+    float denom = fd(1.0f, fa(fa(va, vb), vc));
+    float v = fm(vb, denom), w = fm(vc, denom);
+#pragma unroll
+    for (int k = 0; k < 3; k++) o[k] = fa(fa(a[k], fm(v, ab[k])), fm(w, ac[k]));
+}
+
+__device__ float ray_tri(const float* org, const float* dir, const float* a, const float* b, const float* c) {
+    const float EPS = 1e-6f;
+    float e1[3], e2[3], h[3], sv[3], q[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) { e1[k] = fs(b[k], a[k]); e2[k] = fs(c[k], a[k]); }
+    cross3(dir, e2, h);
+    float aa = dot3(e1, h);
+    if (aa > -EPS && aa < EPS) return -1.f;
+    float f = fd(1.0f, aa);
+#pragma unroll
+    for (int k = 0; k < 3; k++) sv[k] = fs(org[k], a[k]);
+    float u = fm(f, dot3(sv, h));
+    if (u < 0.f || u > 1.f) return -1.f;
+    cross3(sv, e1, q);
+    float v = fm(f, dot3(dir, q));
+    if (v < 0.f || fa(u, v) > 1.f) return -1.f;
+    float t = fm(f, dot3(e2, q));
+    if (t > EPS) return t;
+    return -1.f;
+}
+
+__device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
+    if (S.n_nodes == 0u) return;
+    float mnb[3], mxb[3];
+    xform_point(S.xf, S.cmin, mnb);
+    xform_point(S.xf, S.cmax, mxb);
+    const float margin = S.cmargin;
+    float cur[3], prev[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) { cur[k] = p.pos[k]; prev[k] = fs(cur[k], p.dxp[k]); }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float smin = fs(fminf(mnb[k], mxb[k]), margin);
+        float smax = fa(fmaxf(mnb[k], mxb[k]), margin);
+        if (fminf(cur[k], prev[k]) > smax || fmaxf(cur[k], prev[k]) < smin) return;
+    }
+    if (S.c_nobj == 0u) return;
+
+    float min_d2 = 1e20f;
+    float cnorm[3] = {0.f, 0.f, 1.f}, cpos[3] = {cur[0], cur[1], cur[2]};
+    float min_t = 1.f;
+    float hnorm[3] = {0.f, 0.f, 1.f}, hpos[3] = {cur[0], cur[1], cur[2]};
+    bool has_hit = false;
+    float rd[3] = {p.dxp[0], p.dxp[1], p.dxp[2]};
+    bool do_ccd = len3(rd) > 1e-4f;
+    float curl[3], prevl[3], pminl[3], pmaxl[3];
+    xform_point(S.xfi, cur, curl);
+    xform_point(S.xfi, prev, prevl);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { pminl[k] = fminf(curl[k], prevl[k]); pmaxl[k] = fmaxf(curl[k], prevl[k]); }
+
+    uint32_t stack[32];
+    uint32_t sp = 0;
+    stack[sp++] = 0u;
+    // a well-formed tree visits each node at most once; the cap only ends
+    // traversal of a malformed (cyclic) node array
+    uint32_t visits = 0, max_visits = 2u * S.n_nodes + 64u;
+    while (sp > 0u) {
+        if (++visits > max_visits) { atomicOr(&ctr->status, ST_BVH_STACK); break; }
+        uint32_t ni = stack[--sp];
+        if (ni >= S.n_nodes) continue;
+        const uint4* nd = reinterpret_cast<const uint4*>(S.bvh + (size_t)ni * 8);
+        uint4 n0 = __ldg(nd), n1 = __ldg(nd + 1);
+        float bmin0 = fs(__uint_as_float(n0.x), margin), bmin1 = fs(__uint_as_float(n0.y), margin), bmin2 = fs(__uint_as_float(n0.z), margin);
+        float bmax0 = fa(__uint_as_float(n1.x), margin), bmax1 = fa(__uint_as_float(n1.y), margin), bmax2 = fa(__uint_as_float(n1.z), margin);
+        if (pminl[0] > bmax0 || pminl[1] > bmax1 || pminl[2] > bmax2 ||
+            pmaxl[0] < bmin0 || pmaxl[1] < bmin1 || pmaxl[2] < bmin2) continue;
+        if (n1.w & 0x80000000u) {
+            uint32_t start = n0.w, end = start + (n1.w & 0x7FFFFFFFu);
+            for (uint32_t i = start; i < end; i++) {
+                uint32_t tb = i * 3u;
+                if (tb + 2u >= S.col_words) break;
+                float v0l[3], v1l[3], v2l[3], v0[3], v1[3], v2[3];
+                col_vertex(S, __ldg(&S.col_data[tb]), v0l);
+                col_vertex(S, __ldg(&S.col_data[tb + 1]), v1l);
+                col_vertex(S, __ldg(&S.col_data[tb + 2]), v2l);
+                xform_point(S.xf, v0l, v0);
+                xform_point(S.xf, v1l, v1);
+                xform_point(S.xf, v2l, v2);
+                float cp[3], df[3];
+                closest_point_tri(cur, v0, v1, v2, cp);
+#pragma unroll
+                for (int k = 0; k < 3; k++) df[k] = fs(cur[k], cp[k]);
+                float d2 = dot3(df, df);
+                if (d2 < min_d2) {
+                    min_d2 = d2;
+                    cpos[0] = cp[0]; cpos[1] = cp[1]; cpos[2] = cp[2];
+                    float e1[3], e2[3], n[3];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { e1[k] = fs(v1[k], v0[k]); e2[k] = fs(v2[k], v0[k]); }
+                    cross3(e1, e2, n);
+                    float ln = len3(n);
+                    if (ln > 1e-6f) {
+#pragma unroll
+                        for (int k = 0; k < 3; k++) cnorm[k] = fd(n[k], ln);
+                    }
+                }
+                if (do_ccd) {
+                    float t = ray_tri(prev, rd, v0, v1, v2);
+                    if (t > 0.f && t < min_t) {
+                        min_t = t;
+                        has_hit = true;
+#pragma unroll
+                        for (int k = 0; k < 3; k++) hpos[k] = fa(prev[k], fm(rd[k], t));
+                        float e1[3], e2[3], n[3];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) { e1[k] = fs(v1[k], v0[k]); e2[k] = fs(v2[k], v0[k]); }
+                        cross3(e1, e2, n);
+                        float ln = len3(n);
+                        float fn[3] = {fd(n[0], ln), fd(n[1], ln), fd(n[2], ln)};
+                        float dd = dot3(rd, fn);
+                        float sg = dd > 0.f ? 1.f : (dd < 0.f ? -1.f : 0.f);
+#pragma unroll
+                        for (int k = 0; k < 3; k++) hnorm[k] = fm(fn[k], sg);
+                    }
+                }
+            }
+        } else {
+            if (sp < 31u) {
+                stack[sp++] = n0.w;
+                stack[sp++] = n1.w;
+            } else {
+                atomicOr(&ctr->status, ST_BVH_STACK);
+            }
+        }
+    }
+    float vsf = fd(S.cvs, S.dt);
+    if (has_hit) {
+        float nvv[3], vr[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) p.pos[k] = fa(hpos[k], fm(hnorm[k], S.csurf));
+#pragma unroll
+        for (int k = 0; k < 3; k++) vr[k] = fs(fd(p.dxp[k], S.dt), S.cvel[k]);
+        float vn = dot3(vr, hnorm);
+        float om = fs(1.0f, S.cfric);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float vt = fs(vr[k], fm(vn, hnorm[k]));
+            nvv[k] = vn < 0.f ? fa(fm(vt, om), fm(S.cvel[k], vsf)) : fa(vr[k], fm(S.cvel[k], vsf));
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) { p.vel[k] = nvv[k]; p.dxp[k] = fm(nvv[k], S.dt); }
+        return;
+    }
+    float dist = __fsqrt_rn(min_d2);
+    float df[3], pd[3] = {cnorm[0], cnorm[1], cnorm[2]};
+#pragma unroll
+    for (int k = 0; k < 3; k++) df[k] = fs(cur[k], cpos[k]);
+    float ld = len3(df);
+    if (ld > 1e-6f) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) pd[k] = fd(df[k], ld);
+    }
+    if (dist < S.cthr) {
+        float nvv[3], vr[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) vr[k] = fs(fd(p.dxp[k], S.dt), S.cvel[k]);
+        float vn = dot3(vr, pd);
+        float om = fs(1.0f, 0.0f);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float vt = fs(vr[k], fm(vn, pd[k]));
+            nvv[k] = vn < 0.f ? fa(fm(vt, om), fm(S.cvel[k], vsf)) : fa(vr[k], fm(S.cvel[k], vsf));
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) { p.vel[k] = nvv[k]; p.dxp[k] = fm(nvv[k], S.dt); }
+        if (dist < S.csurf) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) p.pos[k] = fa(cpos[k], fm(pd[k], S.csurf));
+        }
+    }
+}
+
+// integrateParticles (integrateParticles.wgsl:14-72)
+__device__ __forceinline__ void integrate(const SceneDev& S, PState& p, Counters* ctr) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) p.pos[k] = fa(p.pos[k], p.dxp[k]);
+    float IpD[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) IpD[i] = fa((i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f, p.D[i]);
+    mul3(IpD, p.Fe, p.Fe);
+    plasticity(S, p.Fe, p.Fp);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (p.pos[a] < S.gmin[a]) { p.dxp[a] = fm(p.dxp[a], S.rest); p.pos[a] = S.gmin[a]; p.vel[a] = fm(p.vel[a], S.rest); }
+        if (p.pos[a] >= S.gmax[a]) { p.dxp[a] = fm(p.dxp[a], S.rest); p.pos[a] = S.gmax[a]; p.vel[a] = fm(p.vel[a], S.rest); }
+    }
+    collide(S, p, ctr);
+}
+
+// ------------------------------------------------------------------
+// binning kernels
+// ------------------------------------------------------------------
+__global__ void k_clear_table(Ctx c) {
+    uint32_t n = c.counters->n_st;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t s = c.st_slot[i];
+        c.keys[s] = KEY_EMPTY;
+        c.slot_count[s] = 0u;
+    }
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) k_bin_insert(Ctx c) {
+    constexpr int SH = TileGeom<E>::SHIFT;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    bool act = t < c.n_particles;
+    uint64_t key = KEY_EMPTY;
+    uint32_t scene = 0;
+    int st[3] = {0, 0, 0};
+    if (act) {
+        uint32_t p = c.order_in[t];
+        float4 q0 = __ldg(c.particles + (size_t)p * 12);
+        scene = find_scene(c, p);
+        const SceneDev* S = c.scenes + scene;
+        float pos[3] = {q0.x, q0.y, q0.z};
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            int cell = f2i(fd(fs(pos[i], __ldg(&S->gmin[i])), __ldg(&S->cd[i])));
+            int res = __ldg(&S->res[i]);
+            // cells below -1 or above res reach no grid cell; clamping them
+            // only decides which tile processes the particle
+            cell = max(-2, min(cell, res + 1));
+            st[i] = cell >> SH;
+        }
+        key = pack_key(scene, st[0], st[1], st[2]);
+    }
+    unsigned am = __ballot_sync(0xffffffffu, act);
+    if (!act) return;
+    unsigned grp = __match_any_sync(am, key);
+    int leader = __ffs(grp) - 1;
+    int lane = threadIdx.x & 31;
+    uint32_t slot = 0, base = 0;
+    if (lane == leader) {
+        slot = tile_insert(c, key, scene, st[0], st[1], st[2]);
+        base = (slot != INVALID) ? atomicAdd(&c.slot_count[slot], (uint32_t)__popc(grp)) : 0u;
+    }
+    slot = __shfl_sync(grp, slot, leader);
+    base = __shfl_sync(grp, base, leader);
+    c.bin_slot[t] = slot;
+    c.bin_rank[t] = base + (uint32_t)__popc(grp & lanemask_lt());
+}
+
+// per chunk of COMPACT_CHUNK slots: number of occupied slots and particles
+__global__ void __launch_bounds__(256) k_compact_a(Ctx c) {
+    uint32_t base = blockIdx.x * COMPACT_CHUNK + threadIdx.x * 16u;
+    uint32_t ns = 0, np = 0;
+#pragma unroll 4
+    for (int i = 0; i < 16; i++) {
+        if (c.keys[base + i] != KEY_EMPTY) { ns++; np += c.slot_count[base + i]; }
+    }
+    __shared__ uint32_t r_ns[8], r_np[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) { ns += __shfl_xor_sync(0xffffffffu, ns, o); np += __shfl_xor_sync(0xffffffffu, np, o); }
+    if ((threadIdx.x & 31) == 0) { r_ns[threadIdx.x >> 5] = ns; r_np[threadIdx.x >> 5] = np; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t a = 0, b = 0;
+        for (int w = 0; w < 8; w++) { a += r_ns[w]; b += r_np[w]; }
+        c.chunk_nst[blockIdx.x] = a;
+        c.chunk_np[blockIdx.x] = b;
+    }
+}
+
+// exclusive scan of the chunk totals (one block of 1024 threads)
+__global__ void __launch_bounds__(1024) k_compact_b(Ctx c, uint32_t n_chunks) {
+    __shared__ uint32_t s_ns[32], s_np[32];
+    __shared__ uint32_t carry_ns, carry_np;
+    if (threadIdx.x == 0) { carry_ns = 0; carry_np = 0; }
+    __syncthreads();
+    for (uint32_t base = 0; base < n_chunks; base += 1024u) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t vns = i < n_chunks ? c.chunk_nst[i] : 0u;
+        uint32_t vnp = i < n_chunks ? c.chunk_np[i] : 0u;
+        uint32_t ins = vns, inp = vnp;
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t a = __shfl_up_sync(0xffffffffu, ins, o), b = __shfl_up_sync(0xffffffffu, inp, o);
+            if (lane >= o) { ins += a; inp += b; }
+        }
+        if (lane == 31) { s_ns[w] = ins; s_np[w] = inp; }
+        __syncthreads();
+        if (w == 0) {
+            uint32_t a = s_ns[lane], b = s_np[lane];
+            uint32_t xa = a, xb = b;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t ta = __shfl_up_sync(0xffffffffu, xa, o), tb = __shfl_up_sync(0xffffffffu, xb, o);
+                if (lane >= o) { xa += ta; xb += tb; }
+            }
+            s_ns[lane] = xa - a;
+            s_np[lane] = xb - b;
+        }
+        __syncthreads();
+        uint32_t ex_ns = carry_ns + s_ns[w] + ins - vns;
+        uint32_t ex_np = carry_np + s_np[w] + inp - vnp;
+        if (i < n_chunks) { c.chunk_nst[i] = ex_ns; c.chunk_np[i] = ex_np; }
+        __syncthreads();
+        if (threadIdx.x == 1023) { carry_ns = ex_ns + vns; carry_np = ex_np + vnp; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c.counters->n_st = carry_ns;
+        c.counters->n_binned = carry_np;
+        if (carry_ns > c.max_tiles) atomicOr(&c.counters->status, ST_TILE_OVERFLOW);
+    }
+}
+
+// compact tile records in slot order
+__global__ void __launch_bounds__(256) k_compact_c(Ctx c) {
+    uint32_t base = blockIdx.x * COMPACT_CHUNK + threadIdx.x * 16u;
+    uint32_t ns = 0, np = 0;
+    unsigned long long k[16];
+    uint32_t cnt[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        k[i] = c.keys[base + i];
+        cnt[i] = (k[i] != KEY_EMPTY) ? c.slot_count[base + i] : 0u;
+        ns += (k[i] != KEY_EMPTY) ? 1u : 0u;
+        np += cnt[i];
+    }
+    // block exclusive scan of (ns, np)
+    __shared__ uint32_t w_ns[8], w_np[8];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t ins = ns, inp = np;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t a = __shfl_up_sync(0xffffffffu, ins, o), b = __shfl_up_sync(0xffffffffu, inp, o);
+        if (lane >= o) { ins += a; inp += b; }
+    }
+    if (lane == 31) { w_ns[w] = ins; w_np[w] = inp; }
+    __syncthreads();
+    uint32_t pre_ns = c.chunk_nst[blockIdx.x], pre_np = c.chunk_np[blockIdx.x];
+    for (int j = 0; j < w; j++) { pre_ns += w_ns[j]; pre_np += w_np[j]; }
+    uint32_t st = pre_ns + ins - ns;
+    uint32_t off = pre_np + inp - np;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        if (k[i] != KEY_EMPTY) {
+            uint32_t s = base + i;
+            c.slot_st[s] = st;
+            c.slot_off[s] = off;
+            c.st_slot[st] = s;
+            c.st_key[st] = k[i];
+            c.st_begin[st] = off;
+            c.st_count[st] = cnt[i];
+            st++;
+            off += cnt[i];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bin_scatter(Ctx c) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c.n_particles) return;
+    uint32_t slot = c.bin_slot[t];
+    if (slot == INVALID) return;
+    c.sorted[c.slot_off[slot] + c.bin_rank[t]] = c.order_in[t];
+}
+
+// ------------------------------------------------------------------
+// tile helpers
+// ------------------------------------------------------------------
+template <int E>
+struct TileCtx {
+    uint32_t scene;
+    int origin[3];  // first core cell
+    uint64_t key;
+};
+
+template <int E>
+__device__ __forceinline__ void tile_begin(const Ctx& c, uint32_t st, SceneDev& S, TileCtx<E>& T, uint32_t& cur_scene) {
+    uint64_t key = c.st_key[st];
+    uint32_t scene;
+    int sx, sy, sz;
+    unpack_key(key, scene, sx, sy, sz);
+    T.scene = scene;
+    T.key = key;
+    T.origin[0] = sx * E; T.origin[1] = sy * E; T.origin[2] = sz * E;
+    if (scene != cur_scene) {
+        __syncthreads();
+        load_scene_smem(S, c.scenes + scene);
+        cur_scene = scene;
+    }
+}
+
+// sum of all tile halos covering each cell of this tile's (E+2)^3 region
+template <int E>
+__device__ __forceinline__ int4 assemble_cell(const int4* tiles, const int* nbr, int j) {
+    constexpr int H = E + 2, NC = H * H * H;
+    int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
+    int4 s = __ldg(&tiles[(size_t)nbr[13] * NC + j]);
+    int dx0 = lx <= 1 ? -1 : 0, dx1 = lx >= E ? 1 : 0;
+    int dy0 = ly <= 1 ? -1 : 0, dy1 = ly >= E ? 1 : 0;
+    int dz0 = lz <= 1 ? -1 : 0, dz1 = lz >= E ? 1 : 0;
+    for (int dz = dz0; dz <= dz1; dz++)
+        for (int dy = dy0; dy <= dy1; dy++)
+            for (int dx = dx0; dx <= dx1; dx++) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                int t = nbr[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+                if (t < 0) continue;
+                int jj = ((lz - E * dz) * H + (ly - E * dy)) * H + (lx - E * dx);
+                int4 v = __ldg(&tiles[(size_t)t * NC + jj]);
+                s.x = (int)((uint32_t)s.x + (uint32_t)v.x);
+                s.y = (int)((uint32_t)s.y + (uint32_t)v.y);
+                s.z = (int)((uint32_t)s.z + (uint32_t)v.z);
+                s.w = (int)((uint32_t)s.w + (uint32_t)v.w);
+            }
+    return s;
+}
+
+template <int E>
+__device__ __forceinline__ void lookup_neighbors(const Ctx& c, const TileCtx<E>& T, uint32_t st, int* nbr) {
+    if (threadIdx.x < 27) {
+        int d = threadIdx.x;
+        int dx = d % 3 - 1, dy = (d / 3) % 3 - 1, dz = d / 9 - 1;
+        int r;
+        if (d == 13) {
+            r = (int)st;
+        } else {
+            int sx = T.origin[0] / E + dx, sy = T.origin[1] / E + dy, sz = T.origin[2] / E + dz;
+            uint64_t nk = pack_key(T.scene, sx, sy, sz);
+            uint32_t slot = tile_lookup(c, nk, T.scene, sx, sy, sz);
+            r = (slot == INVALID) ? -1 : (int)c.slot_st[slot];
+            if (r >= (int)c.max_tiles) r = -1;
+        }
+        nbr[d] = r;
+    }
+}
+
+// cell velocity used by G2P; explicit mode applies the grid update
+// (gridUpdate.cs.wgsl:15-53) including its i32 round trip first.
+template <bool PB>
+__device__ __forceinline__ void cell_velocity(const SceneDev& S, int4 s, const int* gc, float* v) {
+    bool in = gc[0] >= 0 && gc[1] >= 0 && gc[2] >= 0 && gc[0] < S.res[0] && gc[1] < S.res[1] && gc[2] < S.res[2];
+    float cm = inv_s(S, s.x);
+    if (!in || cm <= 0.0f) { v[0] = 0.f; v[1] = 0.f; v[2] = 0.f; return; }
+    int32_t mi[3] = {s.y, s.z, s.w};
+    if (!PB) {
+        float u[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) u[k] = fa(fd(inv_s(S, mi[k]), cm), fm(S.g[k], S.dt));
+        grid_bc(S, gc, u);
+#pragma unroll
+        for (int k = 0; k < 3; k++) mi[k] = f2i(fm(fm(u[k], cm), S.scale));
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] = fd(inv_s(S, mi[k]), cm);
+    if (PB) grid_bc(S, gc, v);
+}
+
+template <int E, bool PB>
+__device__ __forceinline__ void assemble_velocity_tile(const Ctx& c, const int4* tiles, const SceneDev& S,
+                                                       const TileCtx<E>& T, const int* nbr, float* vel) {
+    constexpr int H = E + 2, NC = H * H * H;
+    for (int j = threadIdx.x; j < NC; j += blockDim.x) {
+        int4 s = assemble_cell<E>(tiles, nbr, j);
+        int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
+        int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
+        float v[3];
+        cell_velocity<PB>(S, s, gc, v);
+        vel[j] = v[0];
+        vel[NC + j] = v[1];
+        vel[2 * NC + j] = v[2];
+    }
+}
+
+// G2P gather from the shared velocity tile (gridToParticle.cs.wgsl:28-130).
+// Cells the reference skips hold velocity 0 here; adding w*0 (+0 or -0) to a
+// running sum that starts at +0 leaves it unchanged, so the sums are equal.
+template <int E, bool PB>
+__device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& T, const float* vel,
+                                           const Stencil& sc, float* nv, float* G) {
+    constexpr int H = E + 2, NC = H * H * H;
+#pragma unroll
+    for (int k = 0; k < 3; k++) nv[k] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 9; i++) G[i] = 0.f;
+    int l0[3];
+    bool inside = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        l0[k] = sc.cell[k] - T.origin[k];
+        inside = inside && l0[k] >= 0 && l0[k] < E;
+    }
+    if (!inside) return;
+    float pcp[3];
+    if (PB) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) pcp[k] = fs(fa(i2f(sc.cell[k]), sc.f[k]), 0.5f);
+    }
+    float dwv[3][3];
+    if (!PB) {
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+            for (int a = 0; a < 3; a++) dwv[k][a] = dwk(k, sc.f[a]);
+    }
+#pragma unroll
+    for (int oz = 0; oz < 3; oz++)
+#pragma unroll
+        for (int oy = 0; oy < 3; oy++)
+#pragma unroll
+            for (int ox = 0; ox < 3; ox++) {
+                int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
+                float cv[3] = {vel[j], vel[NC + j], vel[2 * NC + j]};
+                float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+#pragma unroll
+                for (int k = 0; k < 3; k++) nv[k] = fa(nv[k], fm(wgt, cv[k]));
+                if (!PB) {
+                    float g[3];
+                    g[0] = fm(fm(dwv[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+                    g[1] = fm(fm(sc.w[ox][0], dwv[oy][1]), sc.w[oz][2]);
+                    g[2] = fm(fm(sc.w[ox][0], sc.w[oy][1]), dwv[oz][2]);
+#pragma unroll
+                    for (int col = 0; col < 3; col++)
+#pragma unroll
+                        for (int r = 0; r < 3; r++) G[col * 3 + r] = fa(G[col * 3 + r], fm(g[col], cv[r]));
+                } else {
+                    float wv[3] = {fm(wgt, cv[0]), fm(wgt, cv[1]), fm(wgt, cv[2])};
+                    float dist[3] = {fs(i2f(sc.cell[0] + ox - 1), pcp[0]), fs(i2f(sc.cell[1] + oy - 1), pcp[1]),
+                                     fs(i2f(sc.cell[2] + oz - 1), pcp[2])};
+#pragma unroll
+                    for (int col = 0; col < 3; col++)
+#pragma unroll
+                        for (int r = 0; r < 3; r++) G[col * 3 + r] = fa(G[col * 3 + r], fm(wv[r], dist[col]));
+                }
+            }
+}
+
+template <bool PB>
+__device__ __forceinline__ void g2p_finish(const SceneDev& S, const float* nv, const float* G, PState& p) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) { p.vel[k] = nv[k]; p.dxp[k] = fm(nv[k], S.dt); }
+    if (!PB) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) p.D[i] = fm(G[i], S.dt);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; i++) p.D[i] = fm(fm(G[i], S.dt), 4.0f);
+    }
+}
+
+// affine P2G + particle-side forces (pbmpm.wgsl:41-147) into the shared tile
+template <int E>
+__device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const TileCtx<E>& T, const float* pos, float mass,
+                                                   const float* dxp, const float* D, uint32_t* acc) {
+    constexpr int H = E + 2, NC = H * H * H;
+    Stencil sc;
+    make_stencil(S, pos, sc);
+    int l0[3];
+    bool inside = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        l0[k] = sc.cell[k] - T.origin[k];
+        inside = inside && l0[k] >= 0 && l0[k] < E;
+    }
+    if (!inside) return;
+    float pcp[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) pcp[k] = fs(fa(i2f(sc.cell[k]), sc.f[k]), 0.5f);
+    const bool iact = S.iact != 0u;
+#pragma unroll 1
+    for (int oz = 0; oz < 3; oz++)
+#pragma unroll
+        for (int oy = 0; oy < 3; oy++)
+#pragma unroll
+            for (int ox = 0; ox < 3; ox++) {
+                int cc[3] = {sc.cell[0] + ox - 1, sc.cell[1] + oy - 1, sc.cell[2] + oz - 1};
+                float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+                float wm = fm(wgt, mass);
+                float off[3] = {fs(i2f(cc[0]), pcp[0]), fs(i2f(cc[1]), pcp[1]), fs(i2f(cc[2]), pcp[2])};
+                float aff[3];
+                mv3(D, off, aff);
+                float fo[3] = {S.g[0], S.g[1], S.g[2]};
+                if (iact) {
+                    float dv[3] = {fs(i2f(cc[0]), S.ipos[0]), fs(i2f(cc[1]), S.ipos[1]), fs(i2f(cc[2]), S.ipos[2])};
+                    float dist = len3(dv);
+                    if (dist < S.irad) {
+                        float pd[3] = {0.f, 0.f, 1.f};
+                        float l = len3(dv);
+                        if (l > 0.001f) {
+#pragma unroll
+                            for (int k = 0; k < 3; k++) pd[k] = fd(dv[k], l);
+                        }
+                        float fl = fd(dist, S.irad);
+                        float falloff = fs(1.0f, fm(fl, fl));
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            float af = (S.imode == 0u) ? fm(fm(pd[k], S.istr), falloff)
+                                                       : fm(fm(fm(-pd[k], S.istr), falloff), fs(1.0f, falloff));
+                            fo[k] = fa(fo[k], af);
+                        }
+                    }
+                }
+                int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    float mom = fd(fm(wm, fa(dxp[k], aff[k])), S.dt);
+                    float mc = fm(fm(fd(fo[k], S.fdiv), wm), S.dt);
+                    uint32_t v = (uint32_t)f2i(fm(mom, S.scale)) + (uint32_t)f2i(fm(mc, S.scale));
+                    atomicAdd(&acc[(k + 1) * NC + j], v);
+                }
+                atomicAdd(&acc[j], (uint32_t)f2i(fm(wm, S.scale)));
+            }
+}
+
+template <int E>
+__device__ __forceinline__ void flush_tile(uint32_t* acc, int4* dst) {
+    constexpr int H = E + 2, NC = H * H * H;
+    for (int j = threadIdx.x; j < NC; j += blockDim.x)
+        dst[j] = make_int4((int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j], (int)acc[3 * NC + j]);
+}
+
+template <int E>
+__device__ __forceinline__ void zero_acc(uint32_t* acc) {
+    constexpr int H = E + 2, NC = H * H * H;
+    uint4* a4 = reinterpret_cast<uint4*>(acc);
+    for (int j = threadIdx.x; j < NC; j += blockDim.x) a4[j] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+__device__ __forceinline__ uint32_t n_tiles_now(const Ctx& c) {
+    uint32_t n = c.counters->n_st;
+    return n < c.max_tiles ? n : c.max_tiles;
+}
+
+// ------------------------------------------------------------------
+// explicit P2G (particleToGrid.cs.wgsl:27-79)
+// ------------------------------------------------------------------
+template <int E>
+__global__ void __launch_bounds__(256) k_p2g_explicit(Ctx c) {
+    constexpr int H = E + 2, NC = H * H * H;
+    extern __shared__ uint4 smem_raw[];
+    uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
+    __shared__ SceneDev S;
+    uint32_t cur_scene = INVALID;
+    uint32_t n_st = n_tiles_now(c);
+    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+        TileCtx<E> T;
+        tile_begin<E>(c, st, S, T, cur_scene);
+        zero_acc<E>(acc);
+        __syncthreads();
+        uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            uint32_t pid = c.sorted[begin + i];
+            PState p;
+            load_particle<true>(c.particles + (size_t)pid * 12, p, true, false);
+            Stencil sc;
+            make_stencil(S, p.pos, sc);
+            int l0[3];
+            bool inside = true;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                l0[k] = sc.cell[k] - T.origin[k];
+                inside = inside && l0[k] >= 0 && l0[k] < E;
+            }
+            if (!inside) continue;
+            float M[9];
+            stress_matrix(S, p, M);
+            float pm[3] = {fm(p.mass, p.vel[0]), fm(p.mass, p.vel[1]), fm(p.mass, p.vel[2])};
+            float dw[3][3];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int a = 0; a < 3; a++) dw[k][a] = dwk(k, sc.f[a]);
+#pragma unroll 1
+            for (int oz = 0; oz < 3; oz++)
+#pragma unroll
+                for (int oy = 0; oy < 3; oy++)
+#pragma unroll
+                    for (int ox = 0; ox < 3; ox++) {
+                        float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+                        float g[3];
+                        g[0] = fd(fm(fm(dw[ox][0], sc.w[oy][1]), sc.w[oz][2]), S.cd[0]);
+                        g[1] = fd(fm(fm(sc.w[ox][0], dw[oy][1]), sc.w[oz][2]), S.cd[1]);
+                        g[2] = fd(fm(fm(sc.w[ox][0], sc.w[oy][1]), dw[oz][2]), S.cd[2]);
+                        float sf[3];
+                        mv3(M, g, sf);
+                        int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            float mom = fa(fm(wgt, pm[k]), fm(sf[k], S.dt));
+                            atomicAdd(&acc[(k + 1) * NC + j], (uint32_t)f2i(fm(mom, S.scale)));
+                        }
+                        atomicAdd(&acc[j], (uint32_t)f2i(fm(fm(wgt, p.mass), S.scale)));
+                    }
+        }
+        __syncthreads();
+        flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------
+// G2P + integrate (explicit: gridToParticle.cs.wgsl:28-80; PBMPM :82-130;
+// integrateParticles.wgsl:14-72)
+// ------------------------------------------------------------------
+template <int E, bool PB>
+__global__ void __launch_bounds__(256) k_g2p_integrate(Ctx c) {
+    constexpr int H = E + 2, NC = H * H * H;
+    extern __shared__ uint4 smem_raw[];
+    float* vel = reinterpret_cast<float*>(smem_raw);
+    __shared__ SceneDev S;
+    __shared__ int nbr[27];
+    uint32_t cur_scene = INVALID;
+    uint32_t n_st = n_tiles_now(c);
+    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+        TileCtx<E> T;
+        tile_begin<E>(c, st, S, T, cur_scene);
+        __syncthreads();
+        lookup_neighbors<E>(c, T, st, nbr);
+        __syncthreads();
+        assemble_velocity_tile<E, PB>(c, c.tiles_b, S, T, nbr, vel);
+        __syncthreads();
+        uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            uint32_t pid = c.sorted[begin + i];
+            float4* rec = c.particles + (size_t)pid * 12;
+            PState p;
+            load_particle<false>(rec, p, false, false);
+            Stencil sc;
+            make_stencil(S, p.pos, sc);
+            float nv[3], G[9];
+            g2p_gather<E, PB>(S, T, vel, sc, nv, G);
+            g2p_finish<PB>(S, nv, G, p);
+            integrate(S, p, c.counters);
+            store_particle(rec, p);
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------
+// PBMPM first iteration: constraints + affine P2G + forces
+// (pbmpm.wgsl:154-178)
+// ------------------------------------------------------------------
+template <int E>
+__global__ void __launch_bounds__(256) k_pbmpm_first(Ctx c) {
+    constexpr int H = E + 2, NC = H * H * H;
+    extern __shared__ uint4 smem_raw[];
+    uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
+    __shared__ SceneDev S;
+    uint32_t cur_scene = INVALID;
+    uint32_t n_st = n_tiles_now(c);
+    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+        TileCtx<E> T;
+        tile_begin<E>(c, st, S, T, cur_scene);
+        zero_acc<E>(acc);
+        __syncthreads();
+        uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            uint32_t pid = c.sorted[begin + i];
+            PState p;
+            load_particle<true>(c.particles + (size_t)pid * 12, p, false, true);
+            pbmpm_constraints(S, p.Fe, p.Fp, p.D);
+            p2g_pbmpm_particle<E>(S, T, p.pos, p.mass, p.dxp, p.D, acc);
+        }
+        __syncthreads();
+        flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
+        __syncthreads();
+    }
+}
+
+// PBMPM iteration i>0: G2P of iteration i-1, constraints, P2G of iteration i
+template <int E>
+__global__ void __launch_bounds__(256) k_pbmpm_iter(Ctx c) {
+    constexpr int H = E + 2, NC = H * H * H;
+    extern __shared__ uint4 smem_raw[];
+    uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
+    float* vel = reinterpret_cast<float*>(smem_raw) + 4 * NC;
+    __shared__ SceneDev S;
+    __shared__ int nbr[27];
+    uint32_t cur_scene = INVALID;
+    uint32_t n_st = n_tiles_now(c);
+    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+        TileCtx<E> T;
+        tile_begin<E>(c, st, S, T, cur_scene);
+        __syncthreads();
+        lookup_neighbors<E>(c, T, st, nbr);
+        zero_acc<E>(acc);
+        __syncthreads();
+        assemble_velocity_tile<E, true>(c, c.tiles_b, S, T, nbr, vel);
+        __syncthreads();
+        uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            uint32_t pid = c.sorted[begin + i];
+            PState p;
+            load_particle<true>(c.particles + (size_t)pid * 12, p, false, false);
+            Stencil sc;
+            make_stencil(S, p.pos, sc);
+            float nv[3], G[9];
+            g2p_gather<E, true>(S, T, vel, sc, nv, G);
+            g2p_finish<true>(S, nv, G, p);
+            pbmpm_constraints(S, p.Fe, p.Fp, p.D);
+            p2g_pbmpm_particle<E>(S, T, p.pos, p.mass, p.dxp, p.D, acc);
+        }
+        __syncthreads();
+        flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------
+// dense grid readback for one scene (inspection only)
+// ------------------------------------------------------------------
+template <int E>
+__global__ void __launch_bounds__(256) k_grid_dense(Ctx c, uint32_t scene, int apply_update, int4* out) {
+    constexpr int H = E + 2, NC = H * H * H;
+    __shared__ SceneDev S;
+    __shared__ int nbr[27];
+    uint32_t cur_scene = INVALID;
+    uint32_t n_st = n_tiles_now(c);
+    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+        TileCtx<E> T;
+        tile_begin<E>(c, st, S, T, cur_scene);
+        __syncthreads();
+        if (T.scene != scene) continue;
+        lookup_neighbors<E>(c, T, st, nbr);
+        __syncthreads();
+        for (int j = threadIdx.x; j < NC; j += blockDim.x) {
+            int4 s = assemble_cell<E>(c.tiles_b, nbr, j);
+            int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
+            int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
+            if (gc[0] < 0 || gc[1] < 0 || gc[2] < 0 || gc[0] >= S.res[0] || gc[1] >= S.res[1] || gc[2] >= S.res[2]) continue;
+            if (apply_update) {
+                float cm = inv_s(S, s.x);
+                if (cm > 0.0f) {
+                    int32_t mi[3] = {s.y, s.z, s.w};
+                    float u[3];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) u[k] = fa(fd(inv_s(S, mi[k]), cm), fm(S.g[k], S.dt));
+                    grid_bc(S, gc, u);
+                    s.y = f2i(fm(fm(u[0], cm), S.scale));
+                    s.z = f2i(fm(fm(u[1], cm), S.scale));
+                    s.w = f2i(fm(fm(u[2], cm), S.scale));
+                }
+            }
+            size_t o = ((size_t)gc[2] * S.res[1] + gc[1]) * S.res[0] + gc[0];
+            out[o] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------
+// launch wrappers
+// ------------------------------------------------------------------
+template <int E>
+size_t smem_bytes(uint32_t kid) {
+    constexpr size_t NC = (size_t)(E + 2) * (E + 2) * (E + 2);
+    switch (kid) {
+        case K_P2G_EXPLICIT:
+        case K_PBMPM_FIRST: return 16 * NC;
+        case K_G2P_EXPLICIT:
+        case K_G2P_PBMPM: return 12 * NC;
+        case K_PBMPM_ITER: return 28 * NC;
+        default: return 0;
+    }
+}
+
+template <int E>
+void* kernel_ptr(uint32_t kid) {
+    switch (kid) {
+        case K_BIN_INSERT: return (void*)k_bin_insert<E>;
+        case K_P2G_EXPLICIT: return (void*)k_p2g_explicit<E>;
+        case K_G2P_EXPLICIT: return (void*)k_g2p_integrate<E, false>;
+        case K_PBMPM_FIRST: return (void*)k_pbmpm_first<E>;
+        case K_PBMPM_ITER: return (void*)k_pbmpm_iter<E>;
+        case K_G2P_PBMPM: return (void*)k_g2p_integrate<E, true>;
+        case K_GRID_DENSE: return (void*)k_grid_dense<E>;
+        default: return nullptr;
+    }
+}
+
+template <int E>
+cudaError_t configure_tile_kernels(int* blocks_per_sm) {
+    for (uint32_t kid : {K_P2G_EXPLICIT, K_G2P_EXPLICIT, K_PBMPM_FIRST, K_PBMPM_ITER, K_G2P_PBMPM, K_GRID_DENSE}) {
+        void* f = kernel_ptr<E>(kid);
+        size_t sm = smem_bytes<E>(kid);
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        int nb = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 256, sm);
+        if (e != cudaSuccess) return e;
+        blocks_per_sm[kid] = nb > 0 ? nb : 1;
+    }
+    return cudaSuccess;
+}
+
+template <int E>
+cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_tiles, uint32_t scene, int apply,
+                          int4* out) {
+    uint32_t n = c.n_particles;
+    uint32_t pblocks = (n + 255u) / 256u;
+    uint32_t n_chunks = c.cap / COMPACT_CHUNK;
+    switch (kid) {
+        case K_CLEAR_TABLE: k_clear_table<<<256, 256, 0, s>>>(c); break;
+        case K_BIN_INSERT: if (pblocks) k_bin_insert<E><<<pblocks, 256, 0, s>>>(c); break;
+        case K_COMPACT_A: k_compact_a<<<n_chunks, 256, 0, s>>>(c); break;
+        case K_COMPACT_B: k_compact_b<<<1, 1024, 0, s>>>(c, n_chunks); break;
+        case K_COMPACT_C: k_compact_c<<<n_chunks, 256, 0, s>>>(c); break;
+        case K_BIN_SCATTER: if (pblocks) k_bin_scatter<<<pblocks, 256, 0, s>>>(c); break;
+        case K_P2G_EXPLICIT: k_p2g_explicit<E><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
+        case K_G2P_EXPLICIT: k_g2p_integrate<E, false><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
+        case K_PBMPM_FIRST: k_pbmpm_first<E><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
+        case K_PBMPM_ITER: k_pbmpm_iter<E><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
+        case K_G2P_PBMPM: k_g2p_integrate<E, true><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
+        case K_GRID_DENSE: k_grid_dense<E><<<grid_tiles, 256, 0, s>>>(c, scene, apply, out); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t configure_tile_kernels<8>(int*);
+template cudaError_t configure_tile_kernels<16>(int*);
+template cudaError_t launch_kernel<8>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
+template cudaError_t launch_kernel<16>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
+
+}  // namespace mpm

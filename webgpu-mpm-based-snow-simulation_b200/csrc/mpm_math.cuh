@@ -1,0 +1,212 @@
+// mpm_math.cuh -- device arithmetic of the MPM step.
+//
+// Every helper fixes one evaluation order so the f32 results, and therefore
+// the i32 fixed-point grid, are reproducible bit for bit.  The kernels are
+// compiled with -fmad=false (no contraction of a*b+c), IEEE division and
+// square root, and without flush-to-zero.
+//
+// Conventions (WGSL semantics of the reference shaders):
+//   mat3 is column-major, m[c*3 + r] = M[c][r]; constructors take columns
+//   dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z
+//   (M*v)[r] = (M[0][r]*v.x + M[1][r]*v.y) + M[2][r]*v.z
+//   (A*B)[c][r] = (A[0][r]*B[c][0] + A[1][r]*B[c][1]) + A[2][r]*B[c][2]
+//   det(M) = (M00*(M11*M22 - M21*M12) - M10*(M01*M22 - M21*M02)) + M20*(M01*M12 - M11*M02)
+//   i32(f): truncation toward zero, saturating, NaN -> 0
+//   exp/pow: f64 evaluation by exp64/log64 below, rounded once to f32
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpm {
+
+struct M3 { float m[9]; };
+
+__device__ __forceinline__ int32_t f2i(float x) {
+    return (x != x) ? 0 : __float2int_rz(x);
+}
+__device__ __forceinline__ float i2f(int32_t i) { return __int2float_rn(i); }
+
+// xxHash32-style 3-word mix (randomNumberGenerators.wgsl:24-38).
+__host__ __device__ __forceinline__ uint32_t hash3(uint32_t x, uint32_t y, uint32_t z) {
+    const uint32_t p2 = 2246822519u, p3 = 3266489917u, p4 = 668265263u, p5 = 374761393u;
+    uint32_t h = z + p5 + x * p3;
+    h = p4 * ((h << 17) | (h >> 15));
+    h += y * p3;
+    h = p4 * ((h << 17) | (h >> 15));
+    h = p2 * (h ^ (h >> 15));
+    h = p3 * (h ^ (h >> 13));
+    return h ^ (h >> 16);
+}
+
+// exp(x) in f64: Cody-Waite reduction x = k ln2 + r, then the degree-13
+// Taylor polynomial of e^r (Horner), then exact scaling by 2^k.
+__device__ __forceinline__ double pow2i(int k) {
+    return __longlong_as_double((long long)(k + 1023) << 52);
+}
+__device__ __noinline__ double exp64(double x) {
+    if (x != x) return x;
+    if (x > 709.782712893384) return __longlong_as_double(0x7ff0000000000000ll);
+    if (x < -745.2) return 0.0;
+    const double LN2_HI = 6.93147180369123816490e-01;
+    const double LN2_LO = 1.90821492927058770002e-10;
+    const double INV_LN2 = 1.44269504088896338700e+00;
+    double kf = floor(__dadd_rn(__dmul_rn(x, INV_LN2), 0.5));
+    int k = (int)kf;
+    double r = __dsub_rn(__dsub_rn(x, __dmul_rn(kf, LN2_HI)), __dmul_rn(kf, LN2_LO));
+    double p = 1.0 / 6227020800.0;
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 479001600.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 39916800.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 3628800.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 362880.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 40320.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 5040.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 720.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 120.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 24.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 6.0);
+    p = __dadd_rn(__dmul_rn(p, r), 0.5);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0);
+    int k1 = k / 2, k2 = k - k1;
+    return __dmul_rn(__dmul_rn(p, pow2i(k1)), pow2i(k2));
+}
+
+// log(x) in f64: x = m 2^e, m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s),
+// s = (m-1)/(m+1), odd power series to s^23.
+__device__ __noinline__ double log64(double x) {
+    if (x != x || x < 0.0) return __longlong_as_double(0x7ff8000000000000ll);
+    if (x == 0.0) return __longlong_as_double((long long)0xfff0000000000000ull);
+    if (x == __longlong_as_double(0x7ff0000000000000ll)) return x;
+    int e = 0;
+    unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    if ((u >> 52) == 0) {
+        x = __dmul_rn(x, 18014398509481984.0);
+        u = (unsigned long long)__double_as_longlong(x);
+        e = -54;
+    }
+    e += (int)((u >> 52) & 0x7ff) - 1023;
+    double m = __longlong_as_double((long long)((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull));
+    if (m > 1.4142135623730951) { m = __dmul_rn(m, 0.5); e += 1; }
+    double s = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
+    double s2 = __dmul_rn(s, s);
+    double q = 1.0 / 23.0;
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 21.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 19.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 17.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 15.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 13.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 11.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 9.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 7.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 5.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 3.0);
+    q = __dadd_rn(__dmul_rn(q, s2), 1.0);
+    const double LN2 = 6.93147180559945309417e-01;
+    return __dadd_rn(__dmul_rn((double)e, LN2), __dmul_rn(__dmul_rn(2.0, s), q));
+}
+
+__device__ __forceinline__ float expf_m(float x) { return __double2float_rn(exp64((double)x)); }
+__device__ __forceinline__ float powf_m(float x, float y) {
+    if (x == 0.0f) return y < 0.0f ? __int_as_float(0x7f800000) : (y == 0.0f ? 1.0f : 0.0f);
+    return __double2float_rn(exp64(__dmul_rn((double)y, log64((double)x))));
+}
+
+// ---- scalar f32 ops with explicit rounding (no contraction) ----------
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+__device__ __forceinline__ float dot3(const float* a, const float* b) {
+    return fa(fa(fm(a[0], b[0]), fm(a[1], b[1])), fm(a[2], b[2]));
+}
+__device__ __forceinline__ void cross3(const float* a, const float* b, float* o) {
+    float x = fs(fm(a[1], b[2]), fm(a[2], b[1]));
+    float y = fs(fm(a[2], b[0]), fm(a[0], b[2]));
+    float z = fs(fm(a[0], b[1]), fm(a[1], b[0]));
+    o[0] = x; o[1] = y; o[2] = z;
+}
+__device__ __forceinline__ float len3(const float* a) { return __fsqrt_rn(dot3(a, a)); }
+
+__device__ __forceinline__ float det3(const float* m) {
+    float t0 = fm(m[0], fs(fm(m[4], m[8]), fm(m[7], m[5])));
+    float t1 = fm(m[3], fs(fm(m[1], m[8]), fm(m[7], m[2])));
+    float t2 = fm(m[6], fs(fm(m[1], m[5]), fm(m[4], m[2])));
+    return fa(fs(t0, t1), t2);
+}
+
+// mat3x3Inverse (matrixOps.wgsl:8-27): adjugate * (1/det); identity if det == 0.
+__device__ __forceinline__ void inv3(const float* m, float* o) {
+    float det = det3(m);
+    if (det == 0.0f) {
+        o[0] = 1.f; o[1] = 0.f; o[2] = 0.f; o[3] = 0.f; o[4] = 1.f; o[5] = 0.f; o[6] = 0.f; o[7] = 0.f; o[8] = 1.f;
+        return;
+    }
+    float a0 = fs(fm(m[4], m[8]), fm(m[5], m[7]));
+    float a1 = fs(fm(m[2], m[7]), fm(m[1], m[8]));
+    float a2 = fs(fm(m[1], m[5]), fm(m[2], m[4]));
+    float a3 = fs(fm(m[5], m[6]), fm(m[3], m[8]));
+    float a4 = fs(fm(m[0], m[8]), fm(m[2], m[6]));
+    float a5 = fs(fm(m[2], m[3]), fm(m[0], m[5]));
+    float a6 = fs(fm(m[3], m[7]), fm(m[4], m[6]));
+    float a7 = fs(fm(m[1], m[6]), fm(m[0], m[7]));
+    float a8 = fs(fm(m[0], m[4]), fm(m[1], m[3]));
+    float s = fd(1.0f, det);
+    o[0] = fm(a0, s); o[1] = fm(a1, s); o[2] = fm(a2, s);
+    o[3] = fm(a3, s); o[4] = fm(a4, s); o[5] = fm(a5, s);
+    o[6] = fm(a6, s); o[7] = fm(a7, s); o[8] = fm(a8, s);
+}
+
+__device__ __forceinline__ void tr3(const float* m, float* o) {
+    float t[9] = {m[0], m[3], m[6], m[1], m[4], m[7], m[2], m[5], m[8]};
+#pragma unroll
+    for (int i = 0; i < 9; i++) o[i] = t[i];
+}
+
+__device__ __forceinline__ void mul3(const float* A, const float* B, float* o) {
+    float t[9];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            t[c * 3 + r] = fa(fa(fm(A[r], B[c * 3 + 0]), fm(A[3 + r], B[c * 3 + 1])), fm(A[6 + r], B[c * 3 + 2]));
+#pragma unroll
+    for (int i = 0; i < 9; i++) o[i] = t[i];
+}
+
+__device__ __forceinline__ void mv3(const float* M, const float* v, float* o) {
+    float t0 = fa(fa(fm(M[0], v[0]), fm(M[3], v[1])), fm(M[6], v[2]));
+    float t1 = fa(fa(fm(M[1], v[0]), fm(M[4], v[1])), fm(M[7], v[2]));
+    float t2 = fa(fa(fm(M[2], v[0]), fm(M[5], v[1])), fm(M[8], v[2]));
+    o[0] = t0; o[1] = t1; o[2] = t2;
+}
+
+// calculatePolarDecompositionRotation (matrixOps.wgsl:33-45): 4 averaging
+// steps R <- 0.5 (R + R^-T).
+__device__ __forceinline__ void polar3(const float* F, float* R) {
+    float g[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) g[i] = F[i];
+#pragma unroll 1
+    for (int it = 0; it < 4; it++) {
+        float iv[9];
+        inv3(g, iv);
+        // transpose(iv)[c*3+r] = iv[r*3+c]
+        float t[9] = {iv[0], iv[3], iv[6], iv[1], iv[4], iv[7], iv[2], iv[5], iv[8]};
+#pragma unroll
+        for (int i = 0; i < 9; i++) g[i] = fm(0.5f, fa(g[i], t[i]));
+    }
+#pragma unroll
+    for (int i = 0; i < 9; i++) R[i] = g[i];
+}
+
+// mat4 (column-major) * vec4(v, 1), .xyz
+__device__ __forceinline__ void xform_point(const float* M, const float* v, float* o) {
+    float t[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+        t[r] = fa(fa(fa(fm(M[r], v[0]), fm(M[4 + r], v[1])), fm(M[8 + r], v[2])), fm(M[12 + r], 1.0f));
+    o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
+}
+
+}  // namespace mpm

@@ -1,0 +1,213 @@
+"""Host-side mirror of the reference's MPM plugin surface.
+
+The reference drives its step from TypeScript through three managers:
+  GpuMpmBufferManager      src/lib/gpu/mpm/GpuMpmBufferManager.ts:2-80
+  GpuColliderBufferManager src/lib/gpu/collider/GpuColliderBufferManager.ts:42-351
+  GpuMpmPipelineManager    src/lib/gpu/mpm/GpuMpmPipelineManager.ts:20-521
+and the enum GpuSimulationMethodType (src/lib/gpu/GpuSimulationMethod.ts:1-4).
+The classes below keep those names, arguments and call order; every call
+lands in libmpm.so (include/mpm.h).  Errors raise MpmError (the reference
+surfaces none: WebGPU validation is asynchronous and capacity overflow is
+silently dropped, see mapAffectedBlocks.wgsl:27-31).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+from ._lib import MpmConfig, MpmParams, check, load
+from .layout import PARTICLE_BYTES, PARTICLE_DTYPE, GpuUniformsBufferManager
+
+
+class GpuSimulationMethodType(IntEnum):
+    ExplicitMpm = 0
+    Pbmpm = 1
+
+
+def build_bvh(vertices: np.ndarray, indices: np.ndarray):
+    """Reference-format BVH (GpuColliderBufferManager.ts:222-350) built by
+    libmpm on the host.  Returns (nodes u32 (n, 8), triangle order)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1)
+    idx = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+    nt = idx.size // 3
+    nodes = np.zeros((2 * nt + 1, 8), dtype=np.uint32)
+    order = np.zeros(max(nt, 1), dtype=np.uint32)
+    n = C.c_uint32(0)
+    check(load().mpm_build_bvh(v.ctypes.data, v.size // 3, idx.ctypes.data, idx.size, nodes.ctypes.data,
+                               order.ctypes.data, C.byref(n)))
+    return nodes[: n.value].copy(), order[:nt].copy()
+
+
+class GpuColliderBufferManager:
+    """Packs a collider mesh the way the reference does: one u32 buffer
+    [indices in BVH leaf order | vertices f32x3 | normals | uvs | material
+    indices] plus 32-byte BVH nodes (GpuColliderBufferManager.ts:96-220)."""
+
+    def __init__(self, *, vertices, indices, normals=None, uvs=None, material_indices=None):
+        v = np.asarray(vertices, dtype=np.float32).reshape(-1, 3)
+        idx = np.asarray(indices, dtype=np.uint32).reshape(-1)
+        if v.size:
+            self.min_coords = v.min(axis=0).astype(np.float32)
+            self.max_coords = v.max(axis=0).astype(np.float32)
+        else:
+            self.min_coords = np.full(3, np.inf, np.float32)
+            self.max_coords = np.full(3, -np.inf, np.float32)
+        self.num_indices = int(idx.size)
+        nodes, order = build_bvh(v, idx)
+        self.bvh_nodes = nodes
+        self.num_bvh_nodes = int(nodes.shape[0])
+        tri = idx.reshape(-1, 3)
+        reordered = tri[order[: tri.shape[0]]].reshape(-1) if tri.size else idx
+        parts = [reordered.astype(np.uint32), v.reshape(-1).view(np.uint32)]
+        for extra in (normals, uvs):
+            if extra is not None:
+                parts.append(np.asarray(extra, dtype=np.float32).reshape(-1).view(np.uint32))
+        if material_indices is not None:
+            parts.append(np.asarray(material_indices, dtype=np.uint32).reshape(-1))
+        self.collider_data = np.ascontiguousarray(np.concatenate(parts)) if parts else np.zeros(0, np.uint32)
+        self.indices_offset = 0
+        self.vertices_offset = 4 * self.num_indices
+
+
+class GpuMpmBufferManager:
+    """Owns the libmpm handle and, through it, the particle buffer and the
+    sparse grid storage (GpuMpmBufferManager.ts:15-80).  The grid capacity is
+    sized from the particle count here instead of the reference's fixed
+    500,000 blocks / 2,000,003 hash entries."""
+
+    def __init__(self, *, n_particles: int, device: int = 0, max_scenes: int = 1, tile_edge: int = 16,
+                 max_tiles: int = 0, hash_capacity: int = 0, stream: int | None = None):
+        lib = load()
+        cfg = MpmConfig(max_particles=n_particles, max_scenes=max_scenes, max_tiles=max_tiles,
+                        hash_capacity=hash_capacity, tile_edge=tile_edge, device=device,
+                        stream=C.c_void_p(stream) if stream else None)
+        h = C.c_void_p()
+        rc = lib.mpm_create(C.byref(cfg), C.byref(h))
+        self.handle = h
+        if rc != _lib.MPM_OK:
+            msg = lib.mpm_last_error(h).decode() if h.value else "mpm_create failed"
+            if h.value:
+                lib.mpm_destroy(h)
+            self.handle = None
+            raise _lib.MpmError(rc, msg)
+        self.n_particles = n_particles
+        self.tile_edge = tile_edge
+        self._lib = lib
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.mpm_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # particle buffer (device.queue.writeBuffer / mapAsync equivalents)
+    def write_particles(self, records: np.ndarray) -> None:
+        rec = np.ascontiguousarray(records)
+        assert rec.dtype.itemsize == PARTICLE_BYTES
+        check(self._lib.mpm_set_particles(self.handle, rec.ctypes.data, rec.shape[0], 0), self.handle)
+        self.n_particles = rec.shape[0]
+
+    def write_particles_device(self, dev_ptr: int, n: int) -> None:
+        check(self._lib.mpm_set_particles(self.handle, C.c_void_p(dev_ptr), n, 1), self.handle)
+        self.n_particles = n
+
+    def read_particles(self, n: int | None = None) -> np.ndarray:
+        n = self.n_particles if n is None else n
+        out = np.zeros(n, dtype=PARTICLE_DTYPE)
+        check(self._lib.mpm_get_particles(self.handle, out.ctypes.data, n, 0), self.handle)
+        return out
+
+    def bind_particles_device(self, dev_ptr: int, n: int) -> None:
+        check(self._lib.mpm_bind_particles_device(self.handle, C.c_void_p(dev_ptr), n), self.handle)
+        self.n_particles = n
+
+    def sync(self) -> int:
+        st = C.c_uint32(0)
+        rc = self._lib.mpm_sync(self.handle, C.byref(st))
+        check(rc, self.handle, st.value)
+        return st.value
+
+    def counts(self):
+        a, b = C.c_uint32(0), C.c_uint32(0)
+        check(self._lib.mpm_get_counts(self.handle, C.byref(a), C.byref(b)), self.handle)
+        return a.value, b.value
+
+    def dense_grid(self, res, scene: int = 0, apply_grid_update: bool = False) -> np.ndarray:
+        rx, ry, rz = (int(r) for r in res)
+        out = np.zeros((rz, ry, rx, 4), dtype=np.int32)
+        check(self._lib.mpm_get_grid_dense(self.handle, scene, 1 if apply_grid_update else 0, out.ctypes.data,
+                                           rx * ry * rz), self.handle)
+        return out
+
+
+class GpuMpmPipelineManager:
+    """The step's plugin surface (GpuMpmPipelineManager.ts:42-521).
+
+    Construction wires the uniform block, the extension parameters and the
+    collider into the handle; add_explicit_mpm_dispatches /
+    add_pbmpm_dispatches enqueue one substep each, as the reference's two
+    methods encode one substep's dispatches into a compute pass."""
+
+    def __init__(self, *, mpm_manager: GpuMpmBufferManager, uniforms_manager: GpuUniformsBufferManager,
+                 collider_manager: GpuColliderBufferManager | None = None, params: MpmParams | None = None,
+                 scene: int = 0):
+        self.mpm = mpm_manager
+        self.uniforms = uniforms_manager
+        self.scene = scene
+        self._lib = load()
+        self.params = params if params is not None else _lib.default_params()
+        check(self._lib.mpm_set_params(self.mpm.handle, scene, C.byref(self.params)), self.mpm.handle)
+        if collider_manager is not None:
+            # GpuMpmPipelineManager.ts:80
+            uniforms_manager.write_collider_num_indices(collider_manager.num_indices)
+            cd = collider_manager.collider_data
+            nodes = collider_manager.bvh_nodes
+            check(self._lib.mpm_set_collider(self.mpm.handle, scene, cd.ctypes.data, cd.size,
+                                             collider_manager.num_indices, nodes.ctypes.data, nodes.shape[0]),
+                  self.mpm.handle)
+        self._last_uniforms = None
+        self.push_uniforms()
+
+    def push_uniforms(self) -> None:
+        b = self.uniforms.bytes()
+        if b != self._last_uniforms:
+            check(self._lib.mpm_set_uniforms(self.mpm.handle, self.scene, b, len(b)), self.mpm.handle)
+            self._last_uniforms = b
+
+    def set_params(self, params: MpmParams) -> None:
+        self.params = params
+        check(self._lib.mpm_set_params(self.mpm.handle, self.scene, C.byref(params)), self.mpm.handle)
+
+    def add_explicit_mpm_dispatches(self, *, n_particles: int, hash_map_size: int | None = None,
+                                    n_blocks_in_hash_map: int | None = None) -> None:
+        """GpuMpmPipelineManager.ts:327-428.  hash_map_size and
+        n_blocks_in_hash_map are accepted for signature parity; capacities are
+        fixed when the buffer manager is created."""
+        self.uniforms.write_use_pbmpm(False)
+        self.push_uniforms()
+        check(self._lib.mpm_add_explicit_mpm_dispatches(self.mpm.handle, n_particles), self.mpm.handle)
+
+    def add_pbmpm_dispatches(self, *, n_particles: int, n_blocks_in_hash_map: int | None = None,
+                             hash_map_size: int | None = None) -> None:
+        """GpuMpmPipelineManager.ts:431-521."""
+        self.uniforms.write_use_pbmpm(True)
+        self.push_uniforms()
+        check(self._lib.mpm_add_pbmpm_dispatches(self.mpm.handle, n_particles), self.mpm.handle)
+
+    def step(self, method: GpuSimulationMethodType, n_substeps: int = 1) -> None:
+        self.uniforms.write_use_pbmpm(method == GpuSimulationMethodType.Pbmpm)
+        self.push_uniforms()
+        check(self._lib.mpm_step(self.mpm.handle, int(method), n_substeps), self.mpm.handle)
+
+
+def kernel_names() -> list[str]:
+    lib = load()
+    return [lib.mpm_kernel_name(i).decode() for i in range(lib.mpm_kernel_count())]
