@@ -1,0 +1,380 @@
+"""Benchmark of the MPM substep on B200.
+
+Workload (the configuration the headline metric is quoted on): a snow slab of
+4,194,304 particles (256 x 64 x 256 jittered lattice, spacing 0.003125) over a
+256^2 fBm terrain collider (130,050 triangles, BVH), sparse grid at 512^3
+virtual resolution, dt = 5e-5, PBMPM with 6 constraint iterations.  Inputs
+are seeded synthetic data of those shapes; the particle buffer (805 MB) is
+larger than L2, so no flush is needed between timed steps.
+
+`python bench.py [--gpus N --steps K --warmup W]` prints one JSON line.
+Under torchrun each rank advances its own replica (weak scaling).
+`--impl reference` times the CPU restatement of the reference step (the
+oracle; the reference itself is WGSL that needs a graphics stack) on the
+host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "webgpu-mpm-based-snow-simulation_b200"
+
+METRIC = "particle-substeps/s at 4M (plain vs surrogate, agg err<=1e-3); P2G/G2P HBM GB/s"
+WORKLOAD = "c2_large_pbmpm: 4,194,304-particle snow slab on 130,050-tri fBm terrain, 512^3 sparse grid, PBMPM x6, dt 5e-5"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, mx, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per full-size launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_c2.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def build_scene(pkg, counts=(256, 64, 256)):
+    return pkg.scenes.c2_large_pbmpm(counts=counts)
+
+
+def make_params(pkg, d):
+    p = pkg.default_params()
+    for k, v in d.items():
+        if k == "gravity":
+            p.gravity[:] = [float(x) for x in v]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+# ----------------------------------------------------------------------
+# reference arm: the CPU restatement on the host cores
+# ----------------------------------------------------------------------
+def cpu_reference(steps, warmup, sample_counts=(128, 32, 128)):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the CPU restatement of the reference step (timed CPU baseline)
+
+    pkg = importlib.import_module(PKG)
+    spec = build_scene(pkg, counts=sample_counts)
+    threads = os.cpu_count() or 1
+    oracle.lib().orf_set_threads(threads)
+    n = spec.particles.shape[0]
+    o = oracle.Oracle(n, max_blocks=600000, hash_size=2000003)
+    o.set_collider(*spec.mesh)
+    p = spec.particles.copy()
+    ub = spec.uniforms.bytes()
+    for _ in range(warmup):
+        o.step(ub, spec.params, p, 1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(ub, spec.params, p, 1)
+    dt = time.perf_counter() - t0
+    rate = n * steps / dt
+    sample = (f"{n:,}-particle block of the same slab ({sample_counts[0]}x{sample_counts[1]}x{sample_counts[2]} "
+              f"lattice, same spacing, grid, dt, terrain and PBMPM x6), {steps} substeps")
+    return rate, threads, sample, dt / steps
+
+
+# ----------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------
+def gpu_run(args, rank, world, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module(PKG)
+    lib = pkg.load()
+    spec = build_scene(pkg)
+    n = spec.particles.shape[0]
+    # the library enqueues on this stream; the timing events are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    buf = pkg.GpuMpmBufferManager(n_particles=n, device=local, tile_edge=args.tile_edge, stream=stream.cuda_stream)
+    buf.write_particles(spec.particles)
+    col = pkg.GpuColliderBufferManager(vertices=spec.mesh[0], indices=spec.mesh[1])
+    pipe = pkg.GpuMpmPipelineManager(mpm_manager=buf, uniforms_manager=spec.uniforms, collider_manager=col,
+                                     params=make_params(pkg, spec.params))
+    method = pkg.GpuSimulationMethodType.Pbmpm
+    n_iter = int(spec.params["n_iter"])
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up (also sizes the tile storage from the first binning)
+    for _ in range(args.warmup):
+        pipe.step(method, 1)
+    buf.sync()
+    n_tiles, n_binned = buf.counts()
+
+    # ---- timed region: K substeps, graphs on, events on the launch stream
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        pipe.step(method, 1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    status = buf.sync()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * n * args.steps / (ms * 1e-3)
+
+    # ---- per-kernel times (CUDA events around each launch, same stream)
+    lib.mpm_enable_kernel_timing(buf.handle, 1)
+    kt_steps = max(3, min(args.steps, 10))
+    for _ in range(kt_steps):
+        pipe.step(method, 1)
+    K = lib.mpm_kernel_count()
+    kms = (C.c_float * K)()
+    kcnt = (C.c_uint32 * K)()
+    lib.mpm_kernel_times(buf.handle, kms, kcnt, K)
+    lib.mpm_enable_kernel_timing(buf.handle, 0)
+    names = pkg.kernel_names()
+    kernels = {names[i]: {"ms_per_launch": kms[i] / kcnt[i], "launches_per_step": kcnt[i] // kt_steps}
+               for i in range(K) if kcnt[i]}
+
+    # active cells after the last P2G (grid cells with nonzero mass)
+    grid = buf.dense_grid(spec.res, apply_grid_update=False)
+    n_cells = int((grid[..., 0] != 0).sum())
+    del grid
+
+    # ---- roofline of the dominant kernel (PBMPM iteration: G2P + constraints + P2G)
+    # algorithmic bytes per launch: per particle the fields it needs (pos 12,
+    # mass 4, F_e 36, F_p 36) and its sorted index (4); per active cell one
+    # 16-byte read of the previous grid and one 16-byte write of the new one.
+    peak, peak_kind = measured_peak_hbm()
+    dom = "pbmpm_iter"
+    per_particle, per_cell = 92, 32
+    alg_bytes = n * per_particle + n_cells * per_cell
+    t_launch = kernels[dom]["ms_per_launch"] * 1e-3
+    achieved = alg_bytes / t_launch / 1e9
+    traffic = profile_traffic(dom)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dom,
+                "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    # P2G / G2P halves quoted by the metric: first P2G and the final G2P+integrate
+    p2g_bytes = n * (12 + 4 + 36 + 36 + 12 + 36 + 4) + n_cells * 16
+    g2p_bytes = n_cells * 16 + n * (4 + 88 + 144)
+    p2g_gbs = p2g_bytes / (kernels["pbmpm_first"]["ms_per_launch"] * 1e-3) / 1e9
+    g2p_gbs = g2p_bytes / (kernels["g2p_pbmpm_integrate"]["ms_per_launch"] * 1e-3) / 1e9
+
+    # ---- explicit method on the same state (extra line item)
+    ex = pkg.GpuSimulationMethodType.ExplicitMpm
+    for _ in range(2):
+        pipe.step(ex, 1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ex_steps = max(5, args.steps)
+    for _ in range(ex_steps):
+        pipe.step(ex, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ex_rate = n * ex_steps / (e0.elapsed_time(e1) * 1e-3)
+
+    # ---- end to end through the public API with host buffers
+    host = torch.empty(n * 192, dtype=torch.uint8, pin_memory=True)
+    import numpy as np
+    hv = host.numpy()
+    hv[:] = np.frombuffer(spec.particles.tobytes(), np.uint8)
+    e2e_steps = max(3, min(args.steps, 10))
+    hptr = host.data_ptr()
+
+    def e2e_step():
+        C_ = C
+        pkg._lib.check(lib.mpm_set_particles(buf.handle, C_.c_void_p(hptr), n, 0), buf.handle)
+        pipe.step(method, 1)
+        pkg._lib.check(lib.mpm_get_particles(buf.handle, C_.c_void_p(hptr), n, 0), buf.handle)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_rate = world * n * e2e_steps / e2e_s
+
+    launches_per_step = sum(v["launches_per_step"] for v in kernels.values())
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "particle-substeps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (fixed-point i32 grid)",
+        "data": "synthetic (seeded procedural slab + fBm terrain; no dataset)",
+        "config": {"workload": WORKLOAD, "particles_per_gpu": n, "substeps_timed": args.steps,
+                   "method": "pbmpm", "n_iter": n_iter, "tile_edge": args.tile_edge, "occupied_tiles": n_tiles,
+                   "active_cells": n_cells, "l2": "inputs larger than L2 (805 MB particle buffer)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline,
+        "p2g_gbs": round(p2g_gbs, 1),
+        "g2p_gbs": round(g2p_gbs, 1),
+        "explicit_value": ex_rate,
+        "kernels": {k: round(v["ms_per_launch"], 4) for k, v in kernels.items()},
+        "e2e": {"value": e2e_rate, "unit": "particle-substeps/s", "h2d_bytes_per_step": n * 192,
+                "d2h_bytes_per_step": n * 192},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+        "device_status": status,
+    }
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--tile-edge", type=int, default=16)
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rate, cores, sample, s_step = cpu_reference(max(1, min(args.steps, 2)), 0)
+        line = {"metric": METRIC, "value": rate, "unit": "particle-substeps/s", "n_gpus": args.gpus,
+                "steps": max(1, min(args.steps, 2)), "warmup": 0, "ms_per_step": s_step * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fixed-point i32 grid)",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD},
+                "cpu_baseline": {"value": rate, "unit": "particle-substeps/s", "cores": cores, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": rate, "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = gpu_run(args, rank, world, local)
+    if rank == 0:
+        rate, cores, sample, _ = cpu_reference(args.cpu_steps, 0)
+        out["cpu_baseline"] = {"value": rate, "unit": "particle-substeps/s", "cores": cores, "kind": "port",
+                               "sample": sample}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

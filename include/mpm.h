@@ -58,7 +58,7 @@ typedef struct MpmConfig {
     uint32_t max_scenes;     /* 1 for a single scene */
     uint32_t max_tiles;      /* occupied grid tiles per substep (0: derived) */
     uint32_t hash_capacity;  /* tile hash slots, rounded up to a power of two (0: derived) */
-    uint32_t tile_edge;      /* grid tile edge in cells: 8 or 16 (0: 16) */
+    uint32_t tile_edge;      /* grid tile edge in cells: 8, 12 or 16 (0: 16) */
     int32_t device;          /* CUDA device ordinal */
     void* stream;            /* cudaStream_t to order work on, or NULL for a private stream */
 } MpmConfig;
@@ -91,7 +91,10 @@ typedef struct MpmParams {
 
 /* ---- lifetime ------------------------------------------------------ */
 int mpm_default_params(MpmParams* out);
-/* Allocates every device buffer up front; nothing is allocated per step. */
+/* Allocates the particle and bookkeeping buffers.  Grid-tile storage and the
+ * tile hash table are sized from the first substep's occupancy when
+ * max_tiles / hash_capacity are 0, and grown only inside mpm_sync (between
+ * substeps); a substep itself never allocates. */
 int mpm_create(const MpmConfig* cfg, MpmHandle** out);
 int mpm_destroy(MpmHandle* h);
 const char* mpm_last_error(const MpmHandle* h);
@@ -159,6 +162,13 @@ const char* mpm_kernel_name(uint32_t kernel_id);
 uint32_t mpm_kernel_count(void);
 /* Captures each substep into a CUDA graph (default on). */
 int mpm_use_graphs(MpmHandle* h, int enable);
+/* Device self-test of the step's arithmetic helpers: compares the
+ * corrected-reciprocal division against IEEE division on n pseudo-random
+ * operand pairs and checks the saturating f32->i32 conversion (bit mask of
+ * failed cases).  Both must be 0.  nan_conversion reports the hardware's raw
+ * truncating conversion of a NaN. */
+int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div_mismatches, uint64_t* cvt_mismatches,
+                 uint64_t* nan_conversion);
 
 #ifdef __cplusplus
 }

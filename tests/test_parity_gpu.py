@@ -13,6 +13,16 @@ from helpers import GpuScene, bits_equal, compare_states, run_oracle
 pytestmark = pytest.mark.gpu
 
 
+def test_device_arithmetic_selftest(gpu):
+    """The corrected-reciprocal division equals IEEE division bit for bit on
+    2^28 random operand pairs, and f32->i32 saturates with NaN -> 0."""
+    import ctypes as C
+    a, b, nanv = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+    assert gpu.load().mpm_selftest(0, 1 << 28, 12345, C.byref(a), C.byref(b), C.byref(nanv)) == 0
+    assert a.value == 0, f"{a.value} division mismatches"
+    assert b.value == 0, f"conversion mismatch code {b.value}"
+
+
 def _scene(pkg, **kw):
     return pkg.scenes.parity_scene(**kw)
 

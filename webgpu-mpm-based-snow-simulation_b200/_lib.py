@@ -100,6 +100,8 @@ SIGNATURES = {
     "mpm_kernel_name": (C.c_char_p, [C.c_uint32]),
     "mpm_kernel_count": (C.c_uint32, []),
     "mpm_use_graphs": (C.c_int, [_H, C.c_int]),
+    "mpm_selftest": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                               C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

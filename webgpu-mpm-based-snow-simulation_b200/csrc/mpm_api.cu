@@ -17,11 +17,13 @@
 
 #include "../../include/mpm.h"
 #include "mpm_engine.cuh"
+#include "mpm_math.cuh"
 
 namespace mpm {
 template <int E> cudaError_t configure_tile_kernels(int* blocks_per_sm);
 template <int E> cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_tiles, uint32_t scene,
                                            int apply, int4* out);
+cudaError_t launch_selftest(uint64_t n, uint64_t seed, unsigned long long* counts, cudaStream_t s);
 }  // namespace mpm
 
 using namespace mpm;
@@ -55,6 +57,8 @@ struct MpmHandle {
     uint32_t tile_edge = 16;
     uint32_t cap = 0;
     uint32_t max_tiles = 0;
+    bool auto_tiles = true;   // tile capacity sized from the first binning, grown at sync points
+    bool auto_cap = true;     // hash capacity grown at sync points
 
     float4* particles = nullptr;
     bool own_particles = true;
@@ -97,6 +101,17 @@ struct MpmHandle {
     double kms[K_COUNT] = {0};
     uint32_t kcount[K_COUNT] = {0};
 };
+
+static void destroy_graphs(MpmHandle* h);
+
+static cudaError_t launch_e(uint32_t edge, uint32_t kid, const Ctx& c, cudaStream_t s, int grid, uint32_t scene,
+                            int apply, int4* out) {
+    switch (edge) {
+        case 8: return launch_kernel<8>(kid, c, s, grid, scene, apply, out);
+        case 12: return launch_kernel<12>(kid, c, s, grid, scene, apply, out);
+        default: return launch_kernel<16>(kid, c, s, grid, scene, apply, out);
+    }
+}
 
 static int fail(MpmHandle* h, int code, const char* fmt, ...) {
     if (h) {
@@ -217,12 +232,37 @@ static void build_scene_dev(SceneHost& s) {
     d.bvh = bvh;
     d.col_words = col_words;
     d.n_nodes = n_nodes;
-    // power-of-two fixed-point scale: x / s == x * (1/s) exactly
-    uint32_t sb;
-    std::memcpy(&sb, &d.scale, 4);
-    int ex = (int)((sb >> 23) & 0xff) - 127;
-    d.scale_is_pow2 = ((sb & 0x807fffffu) == 0u && ex >= -100 && ex <= 100) ? 1u : 0u;
-    d.inv_scale = d.scale_is_pow2 ? (float)(1.0 / (double)d.scale) : 0.0f;
+    // Reciprocals of the constant divisors, rounded once in f32 (an IEEE
+    // single division on the host), and the exact division mode each allows.
+    auto mode = [](float v, bool int_valued) -> uint32_t {
+        uint32_t b;
+        std::memcpy(&b, &v, 4);
+        int ex = (int)((b >> 23) & 0xff) - 127;
+        bool pow2 = (b & 0x807fffffu) == 0u && ex > -127 && ex < 128;
+        if (pow2 && ex <= 0) return DIV_POW2;
+        if (pow2 && int_valued && ex <= 100) return DIV_POW2S;
+        float a = std::fabs(v);
+        return (a >= 0x1p-40f && a <= 0x1p40f) ? DIV_CORR : DIV_IEEE;
+    };
+    auto recip = [](float v) { return v != 0.0f ? 1.0f / v : 0.0f; };
+    d.mdt = mode(d.dt, false);
+    d.rdt = recip(d.dt);
+    for (int i = 0; i < 3; i++) {
+        d.mcd[i] = mode(d.cd[i], false);
+        d.rcd[i] = recip(d.cd[i]);
+    }
+    d.mscale = mode(d.scale, true);
+    d.rscale = recip(d.scale);
+    d.mfdiv = mode(d.fdiv, false);
+    d.rfdiv = recip(d.fdiv);
+    // loop-invariant operands of the step, each one IEEE f32 operation
+    // exactly as the kernels would compute it: g / force_divisor
+    // (pbmpm.wgsl:137) and g * dt (gridUpdate.cs.wgsl:44)
+    for (int i = 0; i < 3; i++) {
+        volatile float gi = d.g[i];
+        d.gdiv[i] = gi / d.fdiv;
+        d.gdt[i] = gi * d.dt;
+    }
 }
 
 static void destroy_graphs(MpmHandle* h) {
@@ -258,6 +298,44 @@ extern "C" int mpm_destroy(MpmHandle* h) {
 
 extern "C" const char* mpm_last_error(const MpmHandle* h) { return h ? h->err.c_str() : "null handle"; }
 
+// (Re)allocate the tile hash table for `cap` slots (a power of two >=
+// COMPACT_CHUNK).  Only called between substeps, with the stream idle.
+static int alloc_table(MpmHandle* h, uint32_t cap) {
+    void* old[] = {h->keys, h->slot_count, h->slot_off, h->slot_st, h->st_key, h->st_slot, h->st_begin,
+                   h->st_count, h->chunk_nst, h->chunk_np};
+    for (void* b : old)
+        if (b) cudaFree(b);
+    h->cap = cap;
+    CK(h, cudaMalloc(&h->keys, (size_t)cap * 8));
+    CK(h, cudaMalloc(&h->slot_count, (size_t)cap * 4));
+    CK(h, cudaMalloc(&h->slot_off, (size_t)cap * 4));
+    CK(h, cudaMalloc(&h->slot_st, (size_t)cap * 4));
+    CK(h, cudaMalloc(&h->st_key, (size_t)cap * 8));
+    CK(h, cudaMalloc(&h->st_slot, (size_t)cap * 4));
+    CK(h, cudaMalloc(&h->st_begin, (size_t)cap * 4));
+    CK(h, cudaMalloc(&h->st_count, (size_t)cap * 4));
+    CK(h, cudaMalloc(&h->chunk_nst, (size_t)(cap / COMPACT_CHUNK) * 4));
+    CK(h, cudaMalloc(&h->chunk_np, (size_t)(cap / COMPACT_CHUNK) * 4));
+    CK(h, cudaMemsetAsync(h->keys, 0xff, (size_t)cap * 8, h->stream));
+    CK(h, cudaMemsetAsync(h->slot_count, 0, (size_t)cap * 4, h->stream));
+    // a fresh table holds no slots of a previous substep to clear
+    CK(h, cudaMemsetAsync(&h->counters->n_st, 0, 4, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    destroy_graphs(h);
+    return MPM_OK;
+}
+
+static int alloc_tiles(MpmHandle* h, uint32_t n) {
+    for (int i = 0; i < 2; i++)
+        if (h->tiles[i]) { cudaFree(h->tiles[i]); h->tiles[i] = nullptr; }
+    size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
+    h->max_tiles = n;
+    CK(h, cudaMalloc(&h->tiles[0], (size_t)n * NC * 16));
+    CK(h, cudaMalloc(&h->tiles[1], (size_t)n * NC * 16));
+    destroy_graphs(h);
+    return MPM_OK;
+}
+
 extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     if (!cfg || !out) return MPM_ERR_ARG;
     *out = nullptr;
@@ -266,12 +344,17 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->device = cfg->device;
     if (cfg->max_particles == 0) { *out = h; return fail(h, MPM_ERR_ARG, "max_particles must be > 0"); }
     h->tile_edge = cfg->tile_edge ? cfg->tile_edge : 16u;
-    if (h->tile_edge != 8u && h->tile_edge != 16u) { *out = h; return fail(h, MPM_ERR_ARG, "tile_edge must be 8 or 16"); }
+    if (h->tile_edge != 8u && h->tile_edge != 12u && h->tile_edge != 16u) {
+        *out = h;
+        return fail(h, MPM_ERR_ARG, "tile_edge must be 8, 12 or 16");
+    }
     uint32_t max_scenes = cfg->max_scenes ? cfg->max_scenes : 1u;
     if (max_scenes > 65534u) { *out = h; return fail(h, MPM_ERR_ARG, "max_scenes must be <= 65534"); }
     uint32_t N = cfg->max_particles;
-    h->max_tiles = cfg->max_tiles ? cfg->max_tiles : std::max(1024u, std::min(N / 32u + 64u * max_scenes, 1u << 17));
-    uint32_t cap_req = cfg->hash_capacity ? cfg->hash_capacity : std::max(2u * h->max_tiles, 2u * std::min(N, 1u << 22));
+    h->auto_tiles = cfg->max_tiles == 0;
+    h->max_tiles = cfg->max_tiles;
+    h->auto_cap = cfg->hash_capacity == 0;
+    uint32_t cap_req = cfg->hash_capacity ? cfg->hash_capacity : std::max(4u * cfg->max_tiles, std::min(N, 1u << 20));
     h->cap = std::max(next_pow2(cap_req), (uint32_t)COMPACT_CHUNK);
     *out = h;
 
@@ -284,30 +367,23 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
         CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         h->own_stream = true;
     }
-    size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     CK(h, cudaMalloc(&h->particles, (size_t)N * MPM_PARTICLE_BYTES));
     CK(h, cudaMalloc(&h->order[0], (size_t)N * 4));
     CK(h, cudaMalloc(&h->order[1], (size_t)N * 4));
     CK(h, cudaMalloc(&h->bin_slot, (size_t)N * 4));
     CK(h, cudaMalloc(&h->bin_rank, (size_t)N * 4));
-    CK(h, cudaMalloc(&h->keys, (size_t)h->cap * 8));
-    CK(h, cudaMalloc(&h->slot_count, (size_t)h->cap * 4));
-    CK(h, cudaMalloc(&h->slot_off, (size_t)h->cap * 4));
-    CK(h, cudaMalloc(&h->slot_st, (size_t)h->cap * 4));
-    CK(h, cudaMalloc(&h->st_key, (size_t)h->cap * 8));
-    CK(h, cudaMalloc(&h->st_slot, (size_t)h->cap * 4));
-    CK(h, cudaMalloc(&h->st_begin, (size_t)h->cap * 4));
-    CK(h, cudaMalloc(&h->st_count, (size_t)h->cap * 4));
-    CK(h, cudaMalloc(&h->chunk_nst, (size_t)(h->cap / COMPACT_CHUNK) * 4));
-    CK(h, cudaMalloc(&h->chunk_np, (size_t)(h->cap / COMPACT_CHUNK) * 4));
-    CK(h, cudaMalloc(&h->tiles[0], (size_t)h->max_tiles * NC * 16));
-    CK(h, cudaMalloc(&h->tiles[1], (size_t)h->max_tiles * NC * 16));
     CK(h, cudaMalloc(&h->d_scenes, (size_t)max_scenes * sizeof(SceneDev)));
     CK(h, cudaMalloc(&h->d_scene_first, (size_t)(max_scenes + 1) * 4));
     CK(h, cudaMalloc(&h->counters, sizeof(Counters)));
-    CK(h, cudaMemsetAsync(h->keys, 0xff, (size_t)h->cap * 8, h->stream));
-    CK(h, cudaMemsetAsync(h->slot_count, 0, (size_t)h->cap * 4, h->stream));
     CK(h, cudaMemsetAsync(h->counters, 0, sizeof(Counters), h->stream));
+    {
+        int r = alloc_table(h, h->cap);
+        if (r) return r;
+    }
+    if (!h->auto_tiles) {
+        int r = alloc_tiles(h, h->max_tiles);
+        if (r) return r;
+    }
     CK(h, cudaMemsetAsync(h->particles, 0, (size_t)N * MPM_PARTICLE_BYTES, h->stream));
     h->scenes.resize(max_scenes);
     for (auto& s : h->scenes) {
@@ -318,8 +394,9 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->n_scenes = 1;
     h->scene_first.assign(2, 0);
     h->n_particles = 0;
-    cudaError_t ce = (h->tile_edge == 8u) ? configure_tile_kernels<8>(h->blocks_per_sm)
-                                          : configure_tile_kernels<16>(h->blocks_per_sm);
+    cudaError_t ce = h->tile_edge == 8u    ? configure_tile_kernels<8>(h->blocks_per_sm)
+                     : h->tile_edge == 12u ? configure_tile_kernels<12>(h->blocks_per_sm)
+                                           : configure_tile_kernels<16>(h->blocks_per_sm);
     if (ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "configure kernels: %s", cudaGetErrorString(ce));
     CK(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
@@ -562,8 +639,7 @@ static cudaError_t launch(MpmHandle* h, uint32_t kid, const Ctx& c, bool capturi
         tl.b = get_event(h);
         cudaEventRecord(tl.a, h->stream);
     }
-    cudaError_t e = (h->tile_edge == 8u) ? launch_kernel<8>(kid, c, h->stream, grid, 0, 0, nullptr)
-                                         : launch_kernel<16>(kid, c, h->stream, grid, 0, 0, nullptr);
+    cudaError_t e = launch_e(h->tile_edge, kid, c, h->stream, grid, 0, 0, nullptr);
     if (timed) {
         cudaEventRecord(tl.b, h->stream);
         h->pending.push_back(tl);
@@ -615,11 +691,60 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
     return cudaSuccess;
 }
 
+static int read_counters(MpmHandle* h, Counters* ct) {
+    CK(h, cudaStreamSynchronize(h->stream));
+    CK(h, cudaMemcpy(ct, h->counters, sizeof(*ct), cudaMemcpyDeviceToHost));
+    return MPM_OK;
+}
+
+static uint32_t tiles_for(uint32_t n_st) { return std::max(1024u, n_st + n_st / 2u + 256u); }
+
+// Sizes the automatic capacities from a binning pass over the current
+// particles (no tile data is touched): the hash table to at least four slots
+// per occupied tile, the tile buffers to 1.5x the occupied tiles.
+static int size_from_binning(MpmHandle* h) {
+    for (int attempt = 0; attempt < 4; attempt++) {
+        Ctx c = make_ctx(h, h->order_parity);
+        c.max_tiles = 0xFFFFFFFFu;  // no tile storage is touched by this pass
+        for (uint32_t k : {K_CLEAR_TABLE, K_BIN_INSERT, K_COMPACT_A, K_COMPACT_B, K_COMPACT_C}) {
+            cudaError_t e = launch_e(h->tile_edge, k, c, h->stream, h->n_sms, 0, 0, nullptr);
+            if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "sizing pass: %s", cudaGetErrorString(e));
+        }
+        Counters ct;
+        int r = read_counters(h, &ct);
+        if (r) return r;
+        bool full = (ct.status & ST_HASH_FULL) != 0u;
+        if (h->auto_cap && (full || ct.n_st * 4u > h->cap)) {
+            uint32_t want = next_pow2(std::max(ct.n_st * 8u, h->cap * 4u));
+            uint32_t z = 0;
+            CK(h, cudaMemcpy(&h->counters->status, &z, 4, cudaMemcpyHostToDevice));
+            r = alloc_table(h, want);
+            if (r) return r;
+            continue;
+        }
+        if (full) return fail(h, MPM_ERR_CAPACITY, "tile hash table (%u slots) is full", h->cap);
+        if (h->auto_tiles && (h->tiles[0] == nullptr || ct.n_st > h->max_tiles)) {
+            r = alloc_tiles(h, tiles_for(ct.n_st));
+            if (r) return r;
+        }
+        return MPM_OK;
+    }
+    return fail(h, MPM_ERR_CAPACITY, "tile hash table could not be sized");
+}
+
 static int prepare_step(MpmHandle* h) {
     if (h->n_particles == 0) return fail(h, MPM_ERR_STATE, "no particles");
     cudaSetDevice(h->device);
     int r = upload_scenes(h);
     if (r) return r;
+    if (h->tiles[0] == nullptr) {
+        if (!h->order_valid) {
+            k_iota<<<(h->n_particles + 255) / 256, 256, 0, h->stream>>>(h->order[h->order_parity], h->n_particles);
+            CK(h, cudaGetLastError());
+        }
+        r = size_from_binning(h);
+        if (r) return r;
+    }
     if (!h->order_valid) {
         // both order buffers start as the identity so every entry the next
         // binning pass reads is a valid particle index
@@ -707,11 +832,38 @@ extern "C" int mpm_step_p2g_only(MpmHandle* h, int method) {
 extern "C" int mpm_sync(MpmHandle* h, uint32_t* status_out) {
     if (!h) return MPM_ERR_ARG;
     cudaSetDevice(h->device);
-    CK(h, cudaStreamSynchronize(h->stream));
     Counters ct;
-    CK(h, cudaMemcpy(&ct, h->counters, sizeof(ct), cudaMemcpyDeviceToHost));
+    int r = read_counters(h, &ct);
+    if (r) return r;
     if (status_out) *status_out = ct.status;
+    // grow automatic capacities for the following substeps (stream is idle)
+    if (h->auto_tiles && h->tiles[0] && ct.n_st > h->max_tiles - h->max_tiles / 5u) {
+        r = alloc_tiles(h, tiles_for(ct.n_st));
+        if (r) return r;
+    }
+    if (h->auto_cap && ct.n_st * 4u > h->cap) {
+        r = alloc_table(h, next_pow2(ct.n_st * 8u));
+        if (r) return r;
+    }
     if (ct.status) return fail(h, MPM_ERR_DEVICE_STATUS, "device status 0x%x", ct.status);
+    return MPM_OK;
+}
+
+extern "C" int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div_mismatches, uint64_t* cvt_mismatches,
+                            uint64_t* nan_conversion) {
+    if (cudaSetDevice(device) != cudaSuccess) return MPM_ERR_CUDA;
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, 24) != cudaSuccess) return MPM_ERR_CUDA;
+    unsigned long long hcnt[3] = {0, 0, 0};
+    cudaError_t e = cudaMemset(d, 0, 24);
+    if (e == cudaSuccess) e = launch_selftest(n, seed, d, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(hcnt, d, 24, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return MPM_ERR_CUDA;
+    if (div_mismatches) *div_mismatches = hcnt[0];
+    if (cvt_mismatches) *cvt_mismatches = hcnt[1];
+    if (nan_conversion) *nan_conversion = hcnt[2];
     return MPM_OK;
 }
 
@@ -749,8 +901,7 @@ extern "C" int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_u
     Ctx c = make_ctx(h, h->order_parity);
     c.tiles_b = h->tiles[h->last_tiles];
     int grid = std::max(1, h->n_sms * std::max(1, h->blocks_per_sm[K_GRID_DENSE]));
-    cudaError_t e = (h->tile_edge == 8u) ? launch_kernel<8>(K_GRID_DENSE, c, h->stream, grid, scene, apply_grid_update, dout)
-                                         : launch_kernel<16>(K_GRID_DENSE, c, h->stream, grid, scene, apply_grid_update, dout);
+    cudaError_t e = launch_e(h->tile_edge, K_GRID_DENSE, c, h->stream, grid, scene, apply_grid_update, dout);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out_host, dout, need * 16, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(dout);

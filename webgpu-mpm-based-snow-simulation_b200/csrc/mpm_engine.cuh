@@ -14,7 +14,7 @@
 //   tiles[2]    max_tiles x (E+2)^3 x int4   per-tile halo sums
 //               (mass, momentum x, y, z) in the reference i32 fixed point
 //
-// A tile is E^3 grid cells (E = 8 or 16, i.e. 2^3 or 4^3 of the reference's
+// A tile is E^3 grid cells (E = 8, 12 or 16, i.e. 2^3, 3^3 or 4^3 of the reference's
 // 4^3-cell blocks).  Its P2G writes the (E+2)^3 halo region it touches; the
 // grid value of a cell is the i32 sum over every tile halo that covers it
 // (at most 8), formed on the fly by the G2P kernels.  Integer addition
@@ -37,6 +37,7 @@ constexpr uint32_t ST_TILE_OVERFLOW = 0x2u;
 constexpr uint32_t ST_BVH_STACK = 0x4u;
 constexpr uint32_t ST_SCENE_RANGE = 0x8u;
 constexpr uint32_t ST_MLP_FALLBACK = 0x10u;
+
 
 // Per-scene parameters: the uniform fields the step reads plus the
 // extension constants, laid out for a word-wise copy into shared memory.
@@ -62,9 +63,12 @@ struct SceneDev {
     uint32_t col_words, n_nodes;
     const uint32_t* col_data;
     const uint32_t* bvh;
-    uint32_t scale_is_pow2;
-    float inv_scale;
-    uint32_t pad[2];
+    // host-rounded reciprocals RN(1/d) of the constant divisors and the
+    // division mode (DivMode) each may use
+    float rdt, rcd[3], rscale, rfdiv;
+    float gdiv[3];     // gravity / force_divisor (pbmpm.wgsl:137), exact f32 quotient
+    float gdt[3];      // gravity * dt (gridUpdate.cs.wgsl:44), exact f32 product
+    uint32_t mdt, mcd[3], mscale, mfdiv;
 };
 static_assert(sizeof(SceneDev) % 8 == 0, "SceneDev must be 8-byte sized");
 

@@ -69,12 +69,12 @@ __device__ __forceinline__ uint32_t find_scene(const Ctx& c, uint32_t p) {
     return lo;
 }
 
+// floor(a / E) for a compile-time tile edge E (also for negative a)
 template <int E>
-struct TileGeom {
-    static constexpr int H = E + 2;
-    static constexpr int NC = H * H * H;
-    static constexpr int SHIFT = (E == 8) ? 3 : 4;
-};
+__device__ __forceinline__ int floor_div(int a) {
+    int q = a / E;
+    return (a < 0 && q * E != a) ? q - 1 : q;
+}
 
 __device__ __forceinline__ void load_scene_smem(SceneDev& dst, const SceneDev* src) {
     const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
@@ -83,10 +83,21 @@ __device__ __forceinline__ void load_scene_smem(SceneDev& dst, const SceneDev* s
 }
 
 __device__ __forceinline__ float inv_s(const SceneDev& S, int32_t v) {
-    // f32(i) / fixedPointScale; multiplication by the exact reciprocal when
-    // the scale is a power of two gives the identical f32 result.
-    return S.scale_is_pow2 ? fm(i2f(v), S.inv_scale) : fd(i2f(v), S.scale);
+    // f32(i) / fixedPointScale
+    return divm(i2f(v), S.scale, S.rscale, S.mscale);
 }
+
+// x / m for the three momentum components of one cell: one reciprocal, then
+// the corrected division (bit-identical to x / m) while m is in range.
+struct CellDiv {
+    float m, r;
+    bool fast;
+    __device__ __forceinline__ explicit CellDiv(float mass) : m(mass) {
+        fast = mass >= 0x1p-40f && mass <= 0x1p40f;
+        r = fast ? __frcp_rn(mass) : 0.0f;
+    }
+    __device__ __forceinline__ float operator()(float x) const { return fast ? divc(x, m, r) : __fdiv_rn(x, m); }
+};
 
 // Grid-side boundary of boundary_mode 1 (an extension; the reference only
 // reflects particles): sticky ground plane, slip walls.
@@ -159,13 +170,16 @@ struct Stencil {
     float w[3][3];   // w[k][axis], k = offset + 1
 };
 
+__device__ __forceinline__ float div_cd(const SceneDev& S, float x, int i) { return divm(x, S.cd[i], S.rcd[i], S.mcd[i]); }
+__device__ __forceinline__ float div_dt(const SceneDev& S, float x) { return divm(x, S.dt, S.rdt, S.mdt); }
+
 __device__ __forceinline__ void make_stencil(const SceneDev& S, const float* pos, Stencil& st) {
 #pragma unroll
-    for (int i = 0; i < 3; i++) st.cell[i] = f2i(fd(fs(pos[i], S.gmin[i]), S.cd[i]));
+    for (int i = 0; i < 3; i++) st.cell[i] = f2i(div_cd(S, fs(pos[i], S.gmin[i]), i));
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         float mn = fa(S.gmin[i], fm(S.cd[i], i2f(st.cell[i])));
-        float f = fd(fs(pos[i], mn), S.cd[i]);
+        float f = div_cd(S, fs(pos[i], mn), i);
         st.f[i] = f;
         float om = fs(1.0f, f);
         st.w[0][i] = fm(fm(0.5f, om), om);
@@ -441,7 +455,7 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
 #pragma unroll
         for (int k = 0; k < 3; k++) p.pos[k] = fa(hpos[k], fm(hnorm[k], S.csurf));
 #pragma unroll
-        for (int k = 0; k < 3; k++) vr[k] = fs(fd(p.dxp[k], S.dt), S.cvel[k]);
+        for (int k = 0; k < 3; k++) vr[k] = fs(div_dt(S, p.dxp[k]), S.cvel[k]);
         float vn = dot3(vr, hnorm);
         float om = fs(1.0f, S.cfric);
 #pragma unroll
@@ -465,7 +479,7 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
     if (dist < S.cthr) {
         float nvv[3], vr[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) vr[k] = fs(fd(p.dxp[k], S.dt), S.cvel[k]);
+        for (int k = 0; k < 3; k++) vr[k] = fs(div_dt(S, p.dxp[k]), S.cvel[k]);
         float vn = dot3(vr, pd);
         float om = fs(1.0f, 0.0f);
 #pragma unroll
@@ -513,7 +527,6 @@ __global__ void k_clear_table(Ctx c) {
 
 template <int E>
 __global__ void __launch_bounds__(256) k_bin_insert(Ctx c) {
-    constexpr int SH = TileGeom<E>::SHIFT;
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     bool act = t < c.n_particles;
     uint64_t key = KEY_EMPTY;
@@ -532,7 +545,7 @@ __global__ void __launch_bounds__(256) k_bin_insert(Ctx c) {
             // cells below -1 or above res reach no grid cell; clamping them
             // only decides which tile processes the particle
             cell = max(-2, min(cell, res + 1));
-            st[i] = cell >> SH;
+            st[i] = floor_div<E>(cell);
         }
         key = pack_key(scene, st[0], st[1], st[2]);
     }
@@ -696,7 +709,16 @@ __device__ __forceinline__ void tile_begin(const Ctx& c, uint32_t st, SceneDev& 
     }
 }
 
-// sum of all tile halos covering each cell of this tile's (E+2)^3 region
+__device__ __forceinline__ int4 add4(int4 s, int4 v) {
+    s.x = (int)((uint32_t)s.x + (uint32_t)v.x);
+    s.y = (int)((uint32_t)s.y + (uint32_t)v.y);
+    s.z = (int)((uint32_t)s.z + (uint32_t)v.z);
+    s.w = (int)((uint32_t)s.w + (uint32_t)v.w);
+    return s;
+}
+
+// Sum of all tile halos covering cell j of this tile's (E+2)^3 region, read
+// cell by cell from global memory (inspection kernel only).
 template <int E>
 __device__ __forceinline__ int4 assemble_cell(const int4* tiles, const int* nbr, int j) {
     constexpr int H = E + 2, NC = H * H * H;
@@ -712,11 +734,7 @@ __device__ __forceinline__ int4 assemble_cell(const int4* tiles, const int* nbr,
                 int t = nbr[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
                 if (t < 0) continue;
                 int jj = ((lz - E * dz) * H + (ly - E * dy)) * H + (lx - E * dx);
-                int4 v = __ldg(&tiles[(size_t)t * NC + jj]);
-                s.x = (int)((uint32_t)s.x + (uint32_t)v.x);
-                s.y = (int)((uint32_t)s.y + (uint32_t)v.y);
-                s.z = (int)((uint32_t)s.z + (uint32_t)v.z);
-                s.w = (int)((uint32_t)s.w + (uint32_t)v.w);
+                s = add4(s, __ldg(&tiles[(size_t)t * NC + jj]));
             }
     return s;
 }
@@ -740,40 +758,74 @@ __device__ __forceinline__ void lookup_neighbors(const Ctx& c, const TileCtx<E>&
     }
 }
 
-// cell velocity used by G2P; explicit mode applies the grid update
-// (gridUpdate.cs.wgsl:15-53) including its i32 round trip first.
+// Cell velocity the G2P kernels read.  Explicit mode first applies the grid
+// update (gridUpdate.cs.wgsl:15-53) with its i32 round trip; PBMPM reads the
+// transferred momentum directly (gridToParticle.cs.wgsl:102-108).  Cells the
+// reference skips (outside the grid, or mass <= 0) get velocity 0.
 template <bool PB>
-__device__ __forceinline__ void cell_velocity(const SceneDev& S, int4 s, const int* gc, float* v) {
+__device__ __forceinline__ float4 cell_velocity(const SceneDev& S, int4 s, const int* gc) {
     bool in = gc[0] >= 0 && gc[1] >= 0 && gc[2] >= 0 && gc[0] < S.res[0] && gc[1] < S.res[1] && gc[2] < S.res[2];
     float cm = inv_s(S, s.x);
-    if (!in || cm <= 0.0f) { v[0] = 0.f; v[1] = 0.f; v[2] = 0.f; return; }
+    if (!in || cm <= 0.0f) return make_float4(0.f, 0.f, 0.f, 0.f);
+    CellDiv dm(cm);
     int32_t mi[3] = {s.y, s.z, s.w};
     if (!PB) {
         float u[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) u[k] = fa(fd(inv_s(S, mi[k]), cm), fm(S.g[k], S.dt));
+        for (int k = 0; k < 3; k++) u[k] = fa(dm(inv_s(S, mi[k])), S.gdt[k]);
         grid_bc(S, gc, u);
 #pragma unroll
         for (int k = 0; k < 3; k++) mi[k] = f2i(fm(fm(u[k], cm), S.scale));
     }
+    float v[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) v[k] = fd(inv_s(S, mi[k]), cm);
+    for (int k = 0; k < 3; k++) v[k] = dm(inv_s(S, mi[k]));
     if (PB) grid_bc(S, gc, v);
+    return make_float4(v[0], v[1], v[2], 0.f);
 }
 
+// Assemble this tile's (E+2)^3 cell velocities in shared memory.  Pass 1
+// copies the tile's own halo sums (coalesced 16-byte loads), pass 2 adds
+// the parts of the 26 neighbour halos that overlap this region (shared i32
+// atomics: overlaps of face, edge and corner neighbours coincide), pass 3
+// turns each sum into the velocity in place.
 template <int E, bool PB>
-__device__ __forceinline__ void assemble_velocity_tile(const Ctx& c, const int4* tiles, const SceneDev& S,
-                                                       const TileCtx<E>& T, const int* nbr, float* vel) {
+__device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
+                                                       const int* nbr, int4* cell) {
     constexpr int H = E + 2, NC = H * H * H;
+    const int4* own = tiles + (size_t)nbr[13] * NC;
+    for (int j = threadIdx.x; j < NC; j += blockDim.x) cell[j] = __ldg(own + j);
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < 27; d++) {
+        int t = nbr[d];
+        if (d == 13 || t < 0) continue;
+        // region extents are compile-time constants after unrolling, so the
+        // index decode below uses no runtime integer division
+        const int dx = d % 3 - 1, dy = (d / 3) % 3 - 1, dz = d / 9 - 1;
+        const int x0 = dx > 0 ? E : 0, y0 = dy > 0 ? E : 0, z0 = dz > 0 ? E : 0;
+        const int nx = dx ? 2 : H, ny = dy ? 2 : H, nz = dz ? 2 : H;
+        const int n = nx * ny * nz;
+        const int4* src = tiles + (size_t)t * NC;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            int ix = i % nx, iy = (i / nx) % ny, iz = i / (nx * ny);
+            int lx = x0 + ix, ly = y0 + iy, lz = z0 + iz;
+            int j = (lz * H + ly) * H + lx;
+            int jj = ((lz - E * dz) * H + (ly - E * dy)) * H + (lx - E * dx);
+            int4 v = __ldg(src + jj);
+            int* dst = reinterpret_cast<int*>(&cell[j]);
+            atomicAdd(dst + 0, v.x);
+            atomicAdd(dst + 1, v.y);
+            atomicAdd(dst + 2, v.z);
+            atomicAdd(dst + 3, v.w);
+        }
+    }
+    __syncthreads();
     for (int j = threadIdx.x; j < NC; j += blockDim.x) {
-        int4 s = assemble_cell<E>(tiles, nbr, j);
         int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
         int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
-        float v[3];
-        cell_velocity<PB>(S, s, gc, v);
-        vel[j] = v[0];
-        vel[NC + j] = v[1];
-        vel[2 * NC + j] = v[2];
+        float4 v = cell_velocity<PB>(S, cell[j], gc);
+        reinterpret_cast<float4*>(cell)[j] = v;
     }
 }
 
@@ -781,9 +833,9 @@ __device__ __forceinline__ void assemble_velocity_tile(const Ctx& c, const int4*
 // Cells the reference skips hold velocity 0 here; adding w*0 (+0 or -0) to a
 // running sum that starts at +0 leaves it unchanged, so the sums are equal.
 template <int E, bool PB>
-__device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& T, const float* vel,
+__device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& T, const float4* vel,
                                            const Stencil& sc, float* nv, float* G) {
-    constexpr int H = E + 2, NC = H * H * H;
+    constexpr int H = E + 2;
 #pragma unroll
     for (int k = 0; k < 3; k++) nv[k] = 0.f;
 #pragma unroll
@@ -796,13 +848,16 @@ __device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& 
         inside = inside && l0[k] >= 0 && l0[k] < E;
     }
     if (!inside) return;
-    float pcp[3];
+    float offs[3][3];  // offs[axis][o] = (cell + o - 1) - particle_cell_pos, formed once per axis
+    float dwv[3][3];
     if (PB) {
 #pragma unroll
-        for (int k = 0; k < 3; k++) pcp[k] = fs(fa(i2f(sc.cell[k]), sc.f[k]), 0.5f);
-    }
-    float dwv[3][3];
-    if (!PB) {
+        for (int k = 0; k < 3; k++) {
+            float pcp = fs(fa(i2f(sc.cell[k]), sc.f[k]), 0.5f);
+#pragma unroll
+            for (int o = 0; o < 3; o++) offs[k][o] = fs(i2f(sc.cell[k] + o - 1), pcp);
+        }
+    } else {
 #pragma unroll
         for (int k = 0; k < 3; k++)
 #pragma unroll
@@ -815,23 +870,24 @@ __device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& 
 #pragma unroll
             for (int ox = 0; ox < 3; ox++) {
                 int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
-                float cv[3] = {vel[j], vel[NC + j], vel[2 * NC + j]};
-                float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+                float4 c4 = vel[j];
+                float cv[3] = {c4.x, c4.y, c4.z};
+                float wxy = fm(sc.w[ox][0], sc.w[oy][1]);
+                float wgt = fm(wxy, sc.w[oz][2]);
 #pragma unroll
                 for (int k = 0; k < 3; k++) nv[k] = fa(nv[k], fm(wgt, cv[k]));
                 if (!PB) {
                     float g[3];
                     g[0] = fm(fm(dwv[ox][0], sc.w[oy][1]), sc.w[oz][2]);
                     g[1] = fm(fm(sc.w[ox][0], dwv[oy][1]), sc.w[oz][2]);
-                    g[2] = fm(fm(sc.w[ox][0], sc.w[oy][1]), dwv[oz][2]);
+                    g[2] = fm(wxy, dwv[oz][2]);
 #pragma unroll
                     for (int col = 0; col < 3; col++)
 #pragma unroll
                         for (int r = 0; r < 3; r++) G[col * 3 + r] = fa(G[col * 3 + r], fm(g[col], cv[r]));
                 } else {
                     float wv[3] = {fm(wgt, cv[0]), fm(wgt, cv[1]), fm(wgt, cv[2])};
-                    float dist[3] = {fs(i2f(sc.cell[0] + ox - 1), pcp[0]), fs(i2f(sc.cell[1] + oy - 1), pcp[1]),
-                                     fs(i2f(sc.cell[2] + oz - 1), pcp[2])};
+                    float dist[3] = {offs[0][ox], offs[1][oy], offs[2][oz]};
 #pragma unroll
                     for (int col = 0; col < 3; col++)
 #pragma unroll
@@ -868,24 +924,39 @@ __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const Tile
         inside = inside && l0[k] >= 0 && l0[k] < E;
     }
     if (!inside) return;
-    float pcp[3];
+    // D * off with off = cell - particle_cell_pos; the three column products
+    // of each axis offset are formed once (same operands, same order as the
+    // per-cell matrix-vector product).
+    float pD[3][3][3];  // pD[axis][o][r] = D[axis][r] * off_axis[o]
 #pragma unroll
-    for (int k = 0; k < 3; k++) pcp[k] = fs(fa(i2f(sc.cell[k]), sc.f[k]), 0.5f);
+    for (int a = 0; a < 3; a++) {
+        float pcp = fs(fa(i2f(sc.cell[a]), sc.f[a]), 0.5f);
+#pragma unroll
+        for (int o = 0; o < 3; o++) {
+            float off = fs(i2f(sc.cell[a] + o - 1), pcp);
+#pragma unroll
+            for (int r = 0; r < 3; r++) pD[a][o][r] = fm(D[a * 3 + r], off);
+        }
+    }
     const bool iact = S.iact != 0u;
+    // the z loop stays rolled (code size); its per-z operands are picked by
+    // selects so no array is indexed at run time (which would spill it)
 #pragma unroll 1
-    for (int oz = 0; oz < 3; oz++)
+    for (int oz = 0; oz < 3; oz++) {
+        const float wz = oz == 0 ? sc.w[0][2] : (oz == 1 ? sc.w[1][2] : sc.w[2][2]);
+        float pz[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) pz[k] = oz == 0 ? pD[2][0][k] : (oz == 1 ? pD[2][1][k] : pD[2][2][k]);
 #pragma unroll
         for (int oy = 0; oy < 3; oy++)
 #pragma unroll
             for (int ox = 0; ox < 3; ox++) {
-                int cc[3] = {sc.cell[0] + ox - 1, sc.cell[1] + oy - 1, sc.cell[2] + oz - 1};
-                float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+                float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), wz);
                 float wm = fm(wgt, mass);
-                float off[3] = {fs(i2f(cc[0]), pcp[0]), fs(i2f(cc[1]), pcp[1]), fs(i2f(cc[2]), pcp[2])};
-                float aff[3];
-                mv3(D, off, aff);
-                float fo[3] = {S.g[0], S.g[1], S.g[2]};
+                float fo[3] = {S.gdiv[0], S.gdiv[1], S.gdiv[2]};
                 if (iact) {
+                    int cc[3] = {sc.cell[0] + ox - 1, sc.cell[1] + oy - 1, sc.cell[2] + oz - 1};
+                    float f3[3] = {S.g[0], S.g[1], S.g[2]};
                     float dv[3] = {fs(i2f(cc[0]), S.ipos[0]), fs(i2f(cc[1]), S.ipos[1]), fs(i2f(cc[2]), S.ipos[2])};
                     float dist = len3(dv);
                     if (dist < S.irad) {
@@ -901,20 +972,24 @@ __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const Tile
                         for (int k = 0; k < 3; k++) {
                             float af = (S.imode == 0u) ? fm(fm(pd[k], S.istr), falloff)
                                                        : fm(fm(fm(-pd[k], S.istr), falloff), fs(1.0f, falloff));
-                            fo[k] = fa(fo[k], af);
+                            f3[k] = fa(f3[k], af);
                         }
                     }
+#pragma unroll
+                    for (int k = 0; k < 3; k++) fo[k] = divm(f3[k], S.fdiv, S.rfdiv, S.mfdiv);
                 }
                 int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    float mom = fd(fm(wm, fa(dxp[k], aff[k])), S.dt);
-                    float mc = fm(fm(fd(fo[k], S.fdiv), wm), S.dt);
+                    float aff = fa(fa(pD[0][ox][k], pD[1][oy][k]), pz[k]);
+                    float mom = div_dt(S, fm(wm, fa(dxp[k], aff)));
+                    float mc = fm(fm(fo[k], wm), S.dt);
                     uint32_t v = (uint32_t)f2i(fm(mom, S.scale)) + (uint32_t)f2i(fm(mc, S.scale));
                     atomicAdd(&acc[(k + 1) * NC + j], v);
                 }
                 atomicAdd(&acc[j], (uint32_t)f2i(fm(wm, S.scale)));
             }
+    }
 }
 
 template <int E>
@@ -939,8 +1014,8 @@ __device__ __forceinline__ uint32_t n_tiles_now(const Ctx& c) {
 // ------------------------------------------------------------------
 // explicit P2G (particleToGrid.cs.wgsl:27-79)
 // ------------------------------------------------------------------
-template <int E>
-__global__ void __launch_bounds__(256) k_p2g_explicit(Ctx c) {
+template <int E, int BS>
+__global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
     extern __shared__ uint4 smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
@@ -953,7 +1028,7 @@ __global__ void __launch_bounds__(256) k_p2g_explicit(Ctx c) {
         zero_acc<E>(acc);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
             uint32_t pid = c.sorted[begin + i];
             PState p;
             load_particle<true>(c.particles + (size_t)pid * 12, p, true, false);
@@ -976,16 +1051,19 @@ __global__ void __launch_bounds__(256) k_p2g_explicit(Ctx c) {
 #pragma unroll
                 for (int a = 0; a < 3; a++) dw[k][a] = dwk(k, sc.f[a]);
 #pragma unroll 1
-            for (int oz = 0; oz < 3; oz++)
+            for (int oz = 0; oz < 3; oz++) {
+                const float wz = oz == 0 ? sc.w[0][2] : (oz == 1 ? sc.w[1][2] : sc.w[2][2]);
+                const float dwz = oz == 0 ? dw[0][2] : (oz == 1 ? dw[1][2] : dw[2][2]);
 #pragma unroll
                 for (int oy = 0; oy < 3; oy++)
 #pragma unroll
                     for (int ox = 0; ox < 3; ox++) {
-                        float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), sc.w[oz][2]);
+                        float wxy = fm(sc.w[ox][0], sc.w[oy][1]);
+                        float wgt = fm(wxy, wz);
                         float g[3];
-                        g[0] = fd(fm(fm(dw[ox][0], sc.w[oy][1]), sc.w[oz][2]), S.cd[0]);
-                        g[1] = fd(fm(fm(sc.w[ox][0], dw[oy][1]), sc.w[oz][2]), S.cd[1]);
-                        g[2] = fd(fm(fm(sc.w[ox][0], sc.w[oy][1]), dw[oz][2]), S.cd[2]);
+                        g[0] = div_cd(S, fm(fm(dw[ox][0], sc.w[oy][1]), wz), 0);
+                        g[1] = div_cd(S, fm(fm(sc.w[ox][0], dw[oy][1]), wz), 1);
+                        g[2] = div_cd(S, fm(wxy, dwz), 2);
                         float sf[3];
                         mv3(M, g, sf);
                         int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
@@ -996,6 +1074,7 @@ __global__ void __launch_bounds__(256) k_p2g_explicit(Ctx c) {
                         }
                         atomicAdd(&acc[j], (uint32_t)f2i(fm(fm(wgt, p.mass), S.scale)));
                     }
+            }
         }
         __syncthreads();
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
@@ -1007,11 +1086,13 @@ __global__ void __launch_bounds__(256) k_p2g_explicit(Ctx c) {
 // G2P + integrate (explicit: gridToParticle.cs.wgsl:28-80; PBMPM :82-130;
 // integrateParticles.wgsl:14-72)
 // ------------------------------------------------------------------
-template <int E, bool PB>
-__global__ void __launch_bounds__(256) k_g2p_integrate(Ctx c) {
+template <int E, bool PB, int BS>
+__global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
+    (void)NC;
     extern __shared__ uint4 smem_raw[];
-    float* vel = reinterpret_cast<float*>(smem_raw);
+    int4* cell = reinterpret_cast<int4*>(smem_raw);
+    const float4* vel = reinterpret_cast<const float4*>(smem_raw);
     __shared__ SceneDev S;
     __shared__ int nbr[27];
     uint32_t cur_scene = INVALID;
@@ -1022,10 +1103,10 @@ __global__ void __launch_bounds__(256) k_g2p_integrate(Ctx c) {
         __syncthreads();
         lookup_neighbors<E>(c, T, st, nbr);
         __syncthreads();
-        assemble_velocity_tile<E, PB>(c, c.tiles_b, S, T, nbr, vel);
+        assemble_velocity_tile<E, PB>(c.tiles_b, S, T, nbr, cell);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
             uint32_t pid = c.sorted[begin + i];
             float4* rec = c.particles + (size_t)pid * 12;
             PState p;
@@ -1046,8 +1127,8 @@ __global__ void __launch_bounds__(256) k_g2p_integrate(Ctx c) {
 // PBMPM first iteration: constraints + affine P2G + forces
 // (pbmpm.wgsl:154-178)
 // ------------------------------------------------------------------
-template <int E>
-__global__ void __launch_bounds__(256) k_pbmpm_first(Ctx c) {
+template <int E, int BS>
+__global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
     extern __shared__ uint4 smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
@@ -1060,7 +1141,7 @@ __global__ void __launch_bounds__(256) k_pbmpm_first(Ctx c) {
         zero_acc<E>(acc);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
             uint32_t pid = c.sorted[begin + i];
             PState p;
             load_particle<true>(c.particles + (size_t)pid * 12, p, false, true);
@@ -1074,12 +1155,13 @@ __global__ void __launch_bounds__(256) k_pbmpm_first(Ctx c) {
 }
 
 // PBMPM iteration i>0: G2P of iteration i-1, constraints, P2G of iteration i
-template <int E>
-__global__ void __launch_bounds__(256) k_pbmpm_iter(Ctx c) {
+template <int E, int BS>
+__global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
     extern __shared__ uint4 smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
-    float* vel = reinterpret_cast<float*>(smem_raw) + 4 * NC;
+    int4* cell = reinterpret_cast<int4*>(smem_raw + NC);
+    const float4* vel = reinterpret_cast<const float4*>(smem_raw + NC);
     __shared__ SceneDev S;
     __shared__ int nbr[27];
     uint32_t cur_scene = INVALID;
@@ -1091,10 +1173,10 @@ __global__ void __launch_bounds__(256) k_pbmpm_iter(Ctx c) {
         lookup_neighbors<E>(c, T, st, nbr);
         zero_acc<E>(acc);
         __syncthreads();
-        assemble_velocity_tile<E, true>(c, c.tiles_b, S, T, nbr, vel);
+        assemble_velocity_tile<E, true>(c.tiles_b, S, T, nbr, cell);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
             uint32_t pid = c.sorted[begin + i];
             PState p;
             load_particle<true>(c.particles + (size_t)pid * 12, p, false, false);
@@ -1137,10 +1219,11 @@ __global__ void __launch_bounds__(256) k_grid_dense(Ctx c, uint32_t scene, int a
             if (apply_update) {
                 float cm = inv_s(S, s.x);
                 if (cm > 0.0f) {
+                    CellDiv dm(cm);
                     int32_t mi[3] = {s.y, s.z, s.w};
                     float u[3];
 #pragma unroll
-                    for (int k = 0; k < 3; k++) u[k] = fa(fd(inv_s(S, mi[k]), cm), fm(S.g[k], S.dt));
+                    for (int k = 0; k < 3; k++) u[k] = fa(dm(inv_s(S, mi[k])), S.gdt[k]);
                     grid_bc(S, gc, u);
                     s.y = f2i(fm(fm(u[0], cm), S.scale));
                     s.z = f2i(fm(fm(u[1], cm), S.scale));
@@ -1155,30 +1238,80 @@ __global__ void __launch_bounds__(256) k_grid_dense(Ctx c, uint32_t scene, int a
 }
 
 // ------------------------------------------------------------------
+// device self-test of the arithmetic helpers
+// ------------------------------------------------------------------
+__device__ __forceinline__ uint32_t mix32(uint64_t v) {
+    v ^= v >> 33; v *= 0xff51afd7ed558ccdull; v ^= v >> 33; v *= 0xc4ceb9fe1a85ec53ull; v ^= v >> 33;
+    return (uint32_t)v;
+}
+
+// Compares divc against __fdiv_rn on n pseudo-random operand pairs (random
+// sign, exponent in [-60, 60], mantissa) and checks the f32 -> i32
+// conversion on NaN, infinities and out-of-range values.  counts[0] = division
+// mismatches, counts[1] = conversion mismatches, counts[2] = the raw hardware
+// conversion of a NaN (informational).
+__global__ void k_selftest(uint64_t n, uint64_t seed, unsigned long long* counts) {
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned long long bad = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint32_t a = mix32(seed ^ (i * 2 + 0)), b = mix32(seed ^ (i * 2 + 1));
+        int ex = (int)(a % 121u) - 60, ed = (int)((a >> 8) % 81u) - 40;
+        float x = __uint_as_float((a & 0x80000000u) | ((uint32_t)(ex + 127) << 23) | (b & 0x7fffffu));
+        float d = __uint_as_float(((uint32_t)(ed + 127) << 23) | ((b >> 9) & 0x7fffffu) | ((a & 1u) << 22));
+        if (i & 1) d = -d;
+        float r = __frcp_rn(d);
+        if (__float_as_uint(divc(x, d, r)) != __float_as_uint(__fdiv_rn(x, d))) bad++;
+    }
+    if (bad) atomicAdd(&counts[0], bad);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        volatile float nanv = __int_as_float(0x7fc00000), pinf = __int_as_float(0x7f800000),
+                       ninf = __int_as_float(0xff800000), big = 3e9f, nbig = -3e9f, a = 2.9f, b = -2.9f;
+        unsigned long long cb = 0;
+        if (f2i(nanv) != 0) cb |= 1ull;
+        if (f2i(pinf) != 2147483647) cb |= 2ull;
+        if (f2i(ninf) != (int)0x80000000) cb |= 4ull;
+        if (f2i(big) != 2147483647 || f2i(nbig) != (int)0x80000000) cb |= 8ull;
+        if (f2i(b) != -2 || f2i(a) != 2) cb |= 16ull;
+        counts[1] = cb;
+        counts[2] = (unsigned long long)(uint32_t)__float2int_rz(nanv);
+    }
+}
+
+// ------------------------------------------------------------------
 // launch wrappers
 // ------------------------------------------------------------------
+constexpr int BS_DEFAULT = 256;
+
 template <int E>
 size_t smem_bytes(uint32_t kid) {
     constexpr size_t NC = (size_t)(E + 2) * (E + 2) * (E + 2);
     switch (kid) {
         case K_P2G_EXPLICIT:
-        case K_PBMPM_FIRST: return 16 * NC;
+        case K_PBMPM_FIRST:
         case K_G2P_EXPLICIT:
-        case K_G2P_PBMPM: return 12 * NC;
-        case K_PBMPM_ITER: return 28 * NC;
+        case K_G2P_PBMPM: return 16 * NC;
+        case K_PBMPM_ITER: return 32 * NC;
         default: return 0;
     }
+}
+
+template <int E>
+constexpr int iter_block() { return E == 16 ? 512 : 256; }
+
+template <int E>
+int block_size(uint32_t kid) {
+    return kid == K_PBMPM_ITER ? iter_block<E>() : BS_DEFAULT;
 }
 
 template <int E>
 void* kernel_ptr(uint32_t kid) {
     switch (kid) {
         case K_BIN_INSERT: return (void*)k_bin_insert<E>;
-        case K_P2G_EXPLICIT: return (void*)k_p2g_explicit<E>;
-        case K_G2P_EXPLICIT: return (void*)k_g2p_integrate<E, false>;
-        case K_PBMPM_FIRST: return (void*)k_pbmpm_first<E>;
-        case K_PBMPM_ITER: return (void*)k_pbmpm_iter<E>;
-        case K_G2P_PBMPM: return (void*)k_g2p_integrate<E, true>;
+        case K_P2G_EXPLICIT: return (void*)k_p2g_explicit<E, BS_DEFAULT>;
+        case K_G2P_EXPLICIT: return (void*)k_g2p_integrate<E, false, BS_DEFAULT>;
+        case K_PBMPM_FIRST: return (void*)k_pbmpm_first<E, BS_DEFAULT>;
+        case K_PBMPM_ITER: return (void*)k_pbmpm_iter<E, iter_block<E>()>;
+        case K_G2P_PBMPM: return (void*)k_g2p_integrate<E, true, BS_DEFAULT>;
         case K_GRID_DENSE: return (void*)k_grid_dense<E>;
         default: return nullptr;
     }
@@ -1192,7 +1325,7 @@ cudaError_t configure_tile_kernels(int* blocks_per_sm) {
         cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         int nb = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, 256, sm);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, block_size<E>(kid), sm);
         if (e != cudaSuccess) return e;
         blocks_per_sm[kid] = nb > 0 ? nb : 1;
     }
@@ -1212,20 +1345,27 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
         case K_COMPACT_B: k_compact_b<<<1, 1024, 0, s>>>(c, n_chunks); break;
         case K_COMPACT_C: k_compact_c<<<n_chunks, 256, 0, s>>>(c); break;
         case K_BIN_SCATTER: if (pblocks) k_bin_scatter<<<pblocks, 256, 0, s>>>(c); break;
-        case K_P2G_EXPLICIT: k_p2g_explicit<E><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
-        case K_G2P_EXPLICIT: k_g2p_integrate<E, false><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
-        case K_PBMPM_FIRST: k_pbmpm_first<E><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
-        case K_PBMPM_ITER: k_pbmpm_iter<E><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
-        case K_G2P_PBMPM: k_g2p_integrate<E, true><<<grid_tiles, 256, smem_bytes<E>(kid), s>>>(c); break;
+        case K_P2G_EXPLICIT: k_p2g_explicit<E, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
+        case K_G2P_EXPLICIT: k_g2p_integrate<E, false, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
+        case K_PBMPM_FIRST: k_pbmpm_first<E, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
+        case K_PBMPM_ITER: k_pbmpm_iter<E, iter_block<E>()><<<grid_tiles, iter_block<E>(), smem_bytes<E>(kid), s>>>(c); break;
+        case K_G2P_PBMPM: k_g2p_integrate<E, true, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
         case K_GRID_DENSE: k_grid_dense<E><<<grid_tiles, 256, 0, s>>>(c, scene, apply, out); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
+cudaError_t launch_selftest(uint64_t n, uint64_t seed, unsigned long long* counts, cudaStream_t s) {
+    k_selftest<<<1184, 256, 0, s>>>(n, seed, counts);
+    return cudaGetLastError();
+}
+
 template cudaError_t configure_tile_kernels<8>(int*);
+template cudaError_t configure_tile_kernels<12>(int*);
 template cudaError_t configure_tile_kernels<16>(int*);
 template cudaError_t launch_kernel<8>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
+template cudaError_t launch_kernel<12>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
 template cudaError_t launch_kernel<16>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
 
 }  // namespace mpm

@@ -21,9 +21,9 @@ namespace mpm {
 
 struct M3 { float m[9]; };
 
-__device__ __forceinline__ int32_t f2i(float x) {
-    return (x != x) ? 0 : __float2int_rz(x);
-}
+// cvt.rzi.s32.f32 truncates toward zero, saturates out-of-range values and
+// converts NaN to 0 (checked on the device by mpm_selftest).
+__device__ __forceinline__ int32_t f2i(float x) { return __float2int_rz(x); }
 __device__ __forceinline__ float i2f(int32_t i) { return __int2float_rn(i); }
 
 // xxHash32-style 3-word mix (randomNumberGenerators.wgsl:24-38).
@@ -43,7 +43,7 @@ __host__ __device__ __forceinline__ uint32_t hash3(uint32_t x, uint32_t y, uint3
 __device__ __forceinline__ double pow2i(int k) {
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
-__device__ __noinline__ double exp64(double x) {
+static __device__ __noinline__ double exp64(double x) {
     if (x != x) return x;
     if (x > 709.782712893384) return __longlong_as_double(0x7ff0000000000000ll);
     if (x < -745.2) return 0.0;
@@ -73,7 +73,7 @@ __device__ __noinline__ double exp64(double x) {
 
 // log(x) in f64: x = m 2^e, m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s),
 // s = (m-1)/(m+1), odd power series to s^23.
-__device__ __noinline__ double log64(double x) {
+static __device__ __noinline__ double log64(double x) {
     if (x != x || x < 0.0) return __longlong_as_double(0x7ff8000000000000ll);
     if (x == 0.0) return __longlong_as_double((long long)0xfff0000000000000ull);
     if (x == __longlong_as_double(0x7ff0000000000000ll)) return x;
@@ -116,6 +116,38 @@ __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); 
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+
+// Correctly rounded x / d from the correctly rounded reciprocal r = RN(1/d),
+// for a divisor d in [2^-40, 2^40].  q0 = RN(x r) is within two ulps of x/d;
+// one correction q1 = RN(q0 + (x - d q0) r) makes it faithful; a second
+// correction with the (exact, fused) residual of q1 then returns RN(x/d) by
+// the correction theorem of P. Markstein (IBM J. Res. Dev. 34(1), 1990):
+// a faithful quotient plus a reciprocal within half an ulp give the
+// correctly rounded quotient.  Quotients outside [2^-40, 2^40], zeros,
+// infinities and NaNs take the IEEE division, so no residual can underflow.
+// The result equals __fdiv_rn(x, d) bit for bit; a device self-test checks
+// it on random operands.
+__device__ __forceinline__ float divc(float x, float d, float r) {
+    float q = __fmul_rn(x, r);
+    float a = fabsf(q);
+    if (!(a >= 0x1p-40f && a <= 0x1p40f)) return __fdiv_rn(x, d);
+    float e = __fmaf_rn(-q, d, x);
+    q = __fmaf_rn(e, r, q);
+    e = __fmaf_rn(-q, d, x);
+    return __fmaf_rn(e, r, q);
+}
+// Division modes for a divisor that is constant over a launch:
+//   DIV_IEEE  plain IEEE division
+//   DIV_CORR  corrected reciprocal (divc), |d| in [2^-40, 2^40]
+//   DIV_POW2  d = 2^k with k <= 0: x * 2^-k is exact for every x (scaling by
+//             a power of two >= 1 loses no bits), so it equals x / d
+//   DIV_POW2S d = 2^k with 0 < k <= 100, used only for integer-valued x
+//             (|x| >= 1 or 0): x * 2^-k stays normal, hence exact
+enum DivMode : uint32_t { DIV_IEEE = 0, DIV_CORR = 1, DIV_POW2 = 2, DIV_POW2S = 3 };
+__device__ __forceinline__ float divm(float x, float d, float r, uint32_t mode) {
+    if (mode >= DIV_POW2) return __fmul_rn(x, r);
+    return mode == DIV_CORR ? divc(x, d, r) : __fdiv_rn(x, d);
+}
 
 __device__ __forceinline__ float dot3(const float* a, const float* b) {
     return fa(fa(fm(a[0], b[0]), fm(a[1], b[1])), fm(a[2], b[2]));
