@@ -784,42 +784,114 @@ __device__ __forceinline__ float4 cell_velocity(const SceneDev& S, int4 s, const
     return make_float4(v[0], v[1], v[2], 0.f);
 }
 
-// Assemble this tile's (E+2)^3 cell velocities in shared memory.  Pass 1
-// copies the tile's own halo sums (coalesced 16-byte loads), pass 2 adds
-// the parts of the 26 neighbour halos that overlap this region (shared i32
-// atomics: overlaps of face, edge and corner neighbours coincide), pass 3
-// turns each sum into the velocity in place.
-template <int E, bool PB>
-__device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
-                                                       const int* nbr, int4* cell) {
+// The parts of the 26 neighbour tiles' halos that overlap this tile's
+// (E+2)^3 region, flattened into one index space: 6 face slabs (2 x H x H),
+// then 12 edge bars (2 x 2 x H), then 8 corner cubes (2 x 2 x 2).  Entry e
+// maps to the neighbour direction d (0..26), the cell j of this region and
+// the cell jj of the neighbour's region; every divisor is a compile-time
+// constant.
+template <int E>
+struct HaloEntries {
+    static constexpr int H = E + 2;
+    static constexpr int FACE = 2 * H * H, EDGE = 4 * H;
+    static constexpr int NF = 6 * FACE, NED = 12 * EDGE;
+    static constexpr int N = NF + NED + 64;
+};
+
+template <int E>
+__device__ __forceinline__ void halo_entry(int e, int& d, int& j, int& jj) {
+    constexpr int H = E + 2;
+    using HE = HaloEntries<E>;
+    int dx, dy, dz, ix, iy, iz;
+    if (e < HE::NF) {
+        int r = e / HE::FACE, o = e - r * HE::FACE;
+        int axis = r >> 1, sg = (r & 1) ? 1 : -1;
+        if (axis == 0) { ix = o & 1; iy = (o >> 1) % H; iz = (o >> 1) / H; dx = sg; dy = 0; dz = 0; }
+        else if (axis == 1) { ix = o % H; iy = (o / H) & 1; iz = o / (2 * H); dx = 0; dy = sg; dz = 0; }
+        else { ix = o % H; iy = (o / H) % H; iz = o / (H * H); dx = 0; dy = 0; dz = sg; }
+    } else if (e < HE::NF + HE::NED) {
+        int e2 = e - HE::NF;
+        int r = e2 / HE::EDGE, o = e2 - r * HE::EDGE;
+        int za = r >> 2, s1 = (r & 1) ? 1 : -1, s2 = (r & 2) ? 1 : -1;
+        if (za == 0) { ix = o % H; iy = (o / H) & 1; iz = o / (2 * H); dx = 0; dy = s1; dz = s2; }
+        else if (za == 1) { ix = o & 1; iy = (o >> 1) % H; iz = (o >> 1) / H; dx = s1; dy = 0; dz = s2; }
+        else { ix = o & 1; iy = (o >> 1) & 1; iz = o >> 2; dx = s1; dy = s2; dz = 0; }
+    } else {
+        int o = e - HE::NF - HE::NED;
+        int r = o >> 3;
+        o &= 7;
+        dx = (r & 1) ? 1 : -1; dy = (r & 2) ? 1 : -1; dz = (r & 4) ? 1 : -1;
+        ix = o & 1; iy = (o >> 1) & 1; iz = o >> 2;
+    }
+    int lx = (dx > 0 ? E : 0) + ix, ly = (dy > 0 ? E : 0) + iy, lz = (dz > 0 ? E : 0) + iz;
+    j = (lz * H + ly) * H + lx;
+    jj = ((lz - E * dz) * H + (ly - E * dy)) * H + (lx - E * dx);
+    d = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Sum this tile's halo region: the tile's own (E+2)^3 sums (asynchronous
+// 16-byte copies, all in flight at once) plus the overlapping parts of the
+// neighbour halos (loaded in batches of U per thread before their shared
+// i32 atomic adds, so the loads overlap).  Leaves the int4 sums in `cell`.
+template <int E, int U, bool COPY_MASS = false>
+__device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr, int4* cell,
+                                              uint32_t* own_mass = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
+    constexpr int NE = HaloEntries<E>::N;
     const int4* own = tiles + (size_t)nbr[13] * NC;
-    for (int j = threadIdx.x; j < NC; j += blockDim.x) cell[j] = __ldg(own + j);
+    for (int j = threadIdx.x; j < NC; j += blockDim.x) cp_async16(&cell[j], own + j);
+    cp_async_wait_all();
     __syncthreads();
+    if (COPY_MASS) {
+        // this tile's own halo mass sums, kept before the neighbour sums are added
+        for (int j = threadIdx.x; j < NC; j += blockDim.x) own_mass[j] = (uint32_t)cell[j].x;
+        __syncthreads();
+    }
+    const int step = blockDim.x;
+    for (int base = threadIdx.x; base < NE; base += step * U) {
+        int4 v[U];
+        int jd[U];
 #pragma unroll
-    for (int d = 0; d < 27; d++) {
-        int t = nbr[d];
-        if (d == 13 || t < 0) continue;
-        // region extents are compile-time constants after unrolling, so the
-        // index decode below uses no runtime integer division
-        const int dx = d % 3 - 1, dy = (d / 3) % 3 - 1, dz = d / 9 - 1;
-        const int x0 = dx > 0 ? E : 0, y0 = dy > 0 ? E : 0, z0 = dz > 0 ? E : 0;
-        const int nx = dx ? 2 : H, ny = dy ? 2 : H, nz = dz ? 2 : H;
-        const int n = nx * ny * nz;
-        const int4* src = tiles + (size_t)t * NC;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            int ix = i % nx, iy = (i / nx) % ny, iz = i / (nx * ny);
-            int lx = x0 + ix, ly = y0 + iy, lz = z0 + iz;
-            int j = (lz * H + ly) * H + lx;
-            int jj = ((lz - E * dz) * H + (ly - E * dy)) * H + (lx - E * dx);
-            int4 v = __ldg(src + jj);
-            int* dst = reinterpret_cast<int*>(&cell[j]);
-            atomicAdd(dst + 0, v.x);
-            atomicAdd(dst + 1, v.y);
-            atomicAdd(dst + 2, v.z);
-            atomicAdd(dst + 3, v.w);
+        for (int u = 0; u < U; u++) {
+            int e = base + u * step;
+            jd[u] = -1;
+            v[u] = make_int4(0, 0, 0, 0);
+            if (e < NE) {
+                int d, j, jj;
+                halo_entry<E>(e, d, j, jj);
+                int t = nbr[d];
+                if (t >= 0) {
+                    v[u] = __ldg(tiles + (size_t)t * NC + jj);
+                    jd[u] = j;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (jd[u] >= 0) {
+                int* dst = reinterpret_cast<int*>(&cell[jd[u]]);
+                atomicAdd(dst + 0, v[u].x);
+                atomicAdd(dst + 1, v[u].y);
+                atomicAdd(dst + 2, v[u].z);
+                atomicAdd(dst + 3, v[u].w);
+            }
         }
     }
+}
+
+// Assemble this tile's (E+2)^3 cell velocities in shared memory: halo sums
+// (assemble_sums), then each sum turned into the velocity in place.
+template <int E, bool PB, bool COPY_MASS = false>
+__device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
+                                                       const int* nbr, int4* cell, uint32_t* own_mass = nullptr) {
+    constexpr int H = E + 2, NC = H * H * H;
+    assemble_sums<E, 8, COPY_MASS>(tiles, nbr, cell, own_mass);
     __syncthreads();
     for (int j = threadIdx.x; j < NC; j += blockDim.x) {
         int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
@@ -909,8 +981,11 @@ __device__ __forceinline__ void g2p_finish(const SceneDev& S, const float* nv, c
     }
 }
 
-// affine P2G + particle-side forces (pbmpm.wgsl:41-147) into the shared tile
-template <int E>
+// affine P2G + particle-side forces (pbmpm.wgsl:41-147) into the shared tile.
+// WITH_MASS = false skips the mass adds: within one substep positions and
+// masses do not change between PBMPM iterations, so every iteration's mass
+// sums equal the first iteration's (the caller carries them over).
+template <int E, bool WITH_MASS = true>
 __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const TileCtx<E>& T, const float* pos, float mass,
                                                    const float* dxp, const float* D, uint32_t* acc) {
     constexpr int H = E + 2, NC = H * H * H;
@@ -987,7 +1062,7 @@ __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const Tile
                     uint32_t v = (uint32_t)f2i(fm(mom, S.scale)) + (uint32_t)f2i(fm(mc, S.scale));
                     atomicAdd(&acc[(k + 1) * NC + j], v);
                 }
-                atomicAdd(&acc[j], (uint32_t)f2i(fm(wm, S.scale)));
+                if (WITH_MASS) atomicAdd(&acc[j], (uint32_t)f2i(fm(wm, S.scale)));
             }
     }
 }
@@ -997,6 +1072,12 @@ __device__ __forceinline__ void flush_tile(uint32_t* acc, int4* dst) {
     constexpr int H = E + 2, NC = H * H * H;
     for (int j = threadIdx.x; j < NC; j += blockDim.x)
         dst[j] = make_int4((int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j], (int)acc[3 * NC + j]);
+}
+
+template <int E>
+__device__ __forceinline__ void zero_mom(uint32_t* acc) {
+    constexpr int H = E + 2, NC = H * H * H;
+    for (int j = threadIdx.x; j < 3 * NC; j += blockDim.x) acc[NC + j] = 0u;
 }
 
 template <int E>
@@ -1171,9 +1252,9 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
         tile_begin<E>(c, st, S, T, cur_scene);
         __syncthreads();
         lookup_neighbors<E>(c, T, st, nbr);
-        zero_acc<E>(acc);
+        zero_mom<E>(acc);
         __syncthreads();
-        assemble_velocity_tile<E, true>(c.tiles_b, S, T, nbr, cell);
+        assemble_velocity_tile<E, true, true>(c.tiles_b, S, T, nbr, cell, acc);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1186,7 +1267,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
             g2p_gather<E, true>(S, T, vel, sc, nv, G);
             g2p_finish<true>(S, nv, G, p);
             pbmpm_constraints(S, p.Fe, p.Fp, p.D);
-            p2g_pbmpm_particle<E>(S, T, p.pos, p.mass, p.dxp, p.D, acc);
+            p2g_pbmpm_particle<E, false>(S, T, p.pos, p.mass, p.dxp, p.D, acc);
         }
         __syncthreads();
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
