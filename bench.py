@@ -172,7 +172,7 @@ def gpu_run(args, rank, world, local):
     torch.cuda.set_device(local)
     pkg = importlib.import_module(PKG)
     lib = pkg.load()
-    spec = build_scene(pkg)
+    spec = build_scene(pkg, counts=args.counts)
     n = spec.particles.shape[0]
     # the library enqueues on this stream; the timing events are recorded on it
     stream = torch.cuda.Stream()
@@ -315,7 +315,9 @@ def gpu_run(args, rank, world, local):
         "vs_baseline": None,
         "dtype": "f32 (fixed-point i32 grid)",
         "data": "synthetic (seeded procedural slab + fBm terrain; no dataset)",
-        "config": {"workload": WORKLOAD, "particles_per_gpu": n, "substeps_timed": args.steps,
+        "config": {"workload": WORKLOAD if args.counts == (256, 64, 256) else
+                   f"reduced slab {args.counts[0]}x{args.counts[1]}x{args.counts[2]} of: {WORKLOAD}",
+                   "particles_per_gpu": n, "substeps_timed": args.steps,
                    "method": "pbmpm", "n_iter": n_iter, "tile_edge": args.tile_edge, "occupied_tiles": n_tiles,
                    "active_cells": n_cells, "l2": "inputs larger than L2 (805 MB particle buffer)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -341,7 +343,11 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--tile-edge", type=int, default=16)
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--counts", default="256,64,256",
+                    help="slab lattice size x,y,z (default: the full 4,194,304-particle workload; smaller "
+                         "lattices give the small cases used for profiling)")
     args = ap.parse_args()
+    args.counts = tuple(int(v) for v in args.counts.split(","))
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
 
