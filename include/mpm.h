@@ -170,6 +170,46 @@ int mpm_use_graphs(MpmHandle* h, int enable);
 int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div_mismatches, uint64_t* cvt_mismatches,
                  uint64_t* nan_conversion);
 
+/* ---- allocation-free substep ----------------------------------------
+ * No counterpart in the reference (its TypeScript managers own every GPU
+ * buffer).  For callers that cannot allocate device memory while they run:
+ * a host that hands the library a fixed device-memory budget and owns every
+ * allocation itself (an engine or renderer sharing the GPU through its own
+ * pool), or a real-time frame loop that must not pay cudaMalloc's implicit
+ * device-wide synchronisation.  The caller passes its inputs and outputs
+ * (particle records, collider arrays: device pointers on `device`); every
+ * intermediate buffer of the substep (particle bins, tile hash table, grid
+ * tile sums) lives in one static device array of MPM_NOALLOC_SCRATCH_BYTES
+ * that each GPU loading the library holds until the process exits.  The
+ * call allocates nothing: no cudaMalloc, no cudaFree, no allocating library
+ * routine.
+ *
+ * Limits: at most MPM_NOALLOC_MAX_PARTICLES particles (larger counts are
+ * rejected with MPM_ERR_CAPACITY) and MPM_NOALLOC_MAX_TILES occupied tiles
+ * of MPM_NOALLOC_TILE_EDGE^3 cells (more set status 0x2; tiles past the
+ * limit are skipped).  One scene per call.
+ *
+ * The first call on a device sets the device up (looks up the array's
+ * device address with cudaGetSymbolAddress and configures the kernels);
+ * make that first call before any stream capture.  Every call shares the
+ * one array and clears what must start empty, so calls whose work overlaps
+ * on the GPU (different streams, or other host threads, on one device) race
+ * and must be serialised by the caller.  Work is enqueued on `stream`
+ * (NULL: the legacy default stream).  If status_out is non-NULL the call
+ * waits for the stream, stores the device status bits and returns
+ * MPM_ERR_DEVICE_STATUS when any is set.  err (err_len bytes, may be NULL)
+ * receives a message on failure.  The calling thread's current device is
+ * restored on return. */
+#define MPM_NOALLOC_MAX_PARTICLES 65536u
+#define MPM_NOALLOC_MAX_TILES 512u
+#define MPM_NOALLOC_TILE_EDGE 8u
+#define MPM_NOALLOC_HASH_SLOTS 8192u
+#define MPM_NOALLOC_SCRATCH_BYTES (18u << 20)
+int mpm_step_noalloc(int device, void* stream, void* particles, uint32_t n_particles, int method,
+                     const void* uniforms, size_t uniform_bytes, const MpmParams* params,
+                     const uint32_t* collider_data, size_t collider_words, uint32_t num_indices,
+                     const void* bvh_nodes, uint32_t n_nodes, uint32_t* status_out, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,9 @@ SIGNATURES = {
     "mpm_use_graphs": (C.c_int, [_H, C.c_int]),
     "mpm_selftest": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                C.POINTER(C.c_uint64)]),
+    "mpm_step_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_size_t,
+                                   C.POINTER(MpmParams), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p, C.c_uint32,
+                                   C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]),
 }
 
 _lib = None

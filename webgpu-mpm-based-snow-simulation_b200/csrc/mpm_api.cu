@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -937,5 +938,220 @@ extern "C" int mpm_use_graphs(MpmHandle* h, int enable) {
     if (!h) return MPM_ERR_ARG;
     h->use_graphs = enable != 0;
     if (!h->use_graphs) destroy_graphs(h);
+    return MPM_OK;
+}
+
+// ---------------------------------------------------------------------
+// Allocation-free substep: every intermediate buffer lives in one
+// file-scope device array, so a call allocates no device memory.
+// ---------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t NA_EDGE = 8u;
+constexpr size_t NA_NC = (size_t)(NA_EDGE + 2) * (NA_EDGE + 2) * (NA_EDGE + 2);
+static_assert(MPM_NOALLOC_HASH_SLOTS % COMPACT_CHUNK == 0, "hash slots must be whole compaction chunks");
+static_assert((MPM_NOALLOC_HASH_SLOTS & (MPM_NOALLOC_HASH_SLOTS - 1u)) == 0, "hash slots must be a power of two");
+static_assert(MPM_NOALLOC_TILE_EDGE == NA_EDGE, "header and engine disagree on the tile edge");
+
+constexpr size_t na_round(size_t v) { return (v + 255u) & ~(size_t)255u; }
+constexpr size_t NA_P = MPM_NOALLOC_MAX_PARTICLES, NA_H = MPM_NOALLOC_HASH_SLOTS;
+constexpr size_t NA_ORDER = 0;                                          // particle ids, input order
+constexpr size_t NA_SORTED = NA_ORDER + na_round(NA_P * 4);             // particle ids grouped by tile
+constexpr size_t NA_BIN_SLOT = NA_SORTED + na_round(NA_P * 4);
+constexpr size_t NA_BIN_RANK = NA_BIN_SLOT + na_round(NA_P * 4);
+constexpr size_t NA_KEYS = NA_BIN_RANK + na_round(NA_P * 4);            // tile hash keys (u64)
+constexpr size_t NA_SLOT_COUNT = NA_KEYS + na_round(NA_H * 8);
+constexpr size_t NA_SLOT_OFF = NA_SLOT_COUNT + na_round(NA_H * 4);
+constexpr size_t NA_SLOT_ST = NA_SLOT_OFF + na_round(NA_H * 4);
+constexpr size_t NA_ST_KEY = NA_SLOT_ST + na_round(NA_H * 4);
+constexpr size_t NA_ST_SLOT = NA_ST_KEY + na_round(NA_H * 8);
+constexpr size_t NA_ST_BEGIN = NA_ST_SLOT + na_round(NA_H * 4);
+constexpr size_t NA_ST_COUNT = NA_ST_BEGIN + na_round(NA_H * 4);
+constexpr size_t NA_CHUNK_NST = NA_ST_COUNT + na_round(NA_H * 4);
+constexpr size_t NA_CHUNK_NP = NA_CHUNK_NST + na_round(NA_H / COMPACT_CHUNK * 4);
+constexpr size_t NA_TILES0 = NA_CHUNK_NP + na_round(NA_H / COMPACT_CHUNK * 4);  // halo sums, int4
+constexpr size_t NA_TILES1 = NA_TILES0 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
+constexpr size_t NA_SCENE = NA_TILES1 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
+constexpr size_t NA_SCENE_FIRST = NA_SCENE + na_round(sizeof(SceneDev));
+constexpr size_t NA_COUNTERS = NA_SCENE_FIRST + na_round(2 * 4);
+constexpr size_t NA_BYTES = NA_COUNTERS + na_round(sizeof(Counters));
+static_assert(NA_BYTES <= MPM_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the declared size");
+
+constexpr int NA_MAX_DEVICES = 64;
+
+struct NaDevice {
+    bool ready = false;
+    unsigned char* base = nullptr;  // device address of the scratch array on this device
+    int n_sms = 0;
+    int blocks_per_sm[K_COUNT] = {0};
+};
+
+std::mutex g_na_mutex;
+NaDevice g_na_dev[NA_MAX_DEVICES];
+
+int na_fail(char* err, size_t err_len, int code, const char* fmt, ...) {
+    if (err && err_len) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(err, err_len, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+}  // namespace
+
+// The scratch itself.  A host-side use of this name refers to a host stand-in,
+// not to device memory: host code passes kernels the address returned by
+// cudaGetSymbolAddress for the current device instead.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MPM_NOALLOC_SCRATCH_BYTES];
+
+extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint32_t n_particles, int method,
+                                const void* uniforms, size_t uniform_bytes, const MpmParams* params,
+                                const uint32_t* collider_data, size_t collider_words, uint32_t num_indices,
+                                const void* bvh_nodes, uint32_t n_nodes, uint32_t* status_out, char* err,
+                                size_t err_len) {
+    if (err && err_len) err[0] = '\0';
+    if (!particles || n_particles == 0) return na_fail(err, err_len, MPM_ERR_ARG, "no particle buffer");
+    if (n_particles > MPM_NOALLOC_MAX_PARTICLES)
+        return na_fail(err, err_len, MPM_ERR_CAPACITY, "%u particles exceed the allocation-free limit of %u",
+                       n_particles, MPM_NOALLOC_MAX_PARTICLES);
+    if (((uintptr_t)particles & 15u) != 0) return na_fail(err, err_len, MPM_ERR_ARG, "particle buffer must be 16-byte aligned");
+    if (method != MPM_METHOD_EXPLICIT && method != MPM_METHOD_PBMPM)
+        return na_fail(err, err_len, MPM_ERR_ARG, "bad method %d", method);
+    if (!uniforms || uniform_bytes < 544)
+        return na_fail(err, err_len, MPM_ERR_ARG, "uniform block needs >= 544 bytes, got %zu", uniform_bytes);
+    if (!params || params->n_iter == 0) return na_fail(err, err_len, MPM_ERR_ARG, "params missing or n_iter == 0");
+    if ((collider_words && !collider_data) || (n_nodes && !bvh_nodes))
+        return na_fail(err, err_len, MPM_ERR_ARG, "null collider buffer");
+    if ((size_t)num_indices > collider_words)
+        return na_fail(err, err_len, MPM_ERR_ARG, "num_indices %u > collider words %zu", num_indices, collider_words);
+    if (device < 0 || device >= NA_MAX_DEVICES) return na_fail(err, err_len, MPM_ERR_ARG, "device %d out of range", device);
+
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return na_fail(err, err_len, MPM_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    struct Restore {
+        int d;
+        ~Restore() { if (d >= 0) cudaSetDevice(d); }
+    } restore{prev};
+
+    // once per device, with that device current: the scratch array's device
+    // address and the tile kernels' launch configuration
+    NaDevice& D = g_na_dev[device];
+    {
+        std::lock_guard<std::mutex> lock(g_na_mutex);
+        if (!D.ready) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess)
+                return na_fail(err, err_len, MPM_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            e = cudaDeviceGetAttribute(&D.n_sms, cudaDevAttrMultiProcessorCount, device);
+            if (e != cudaSuccess) return na_fail(err, err_len, MPM_ERR_CUDA, "SM count: %s", cudaGetErrorString(e));
+            e = configure_tile_kernels<NA_EDGE>(D.blocks_per_sm);
+            if (e != cudaSuccess)
+                return na_fail(err, err_len, MPM_ERR_CUDA, "configure kernels: %s", cudaGetErrorString(e));
+            D.base = (unsigned char*)p;
+            D.ready = true;
+        }
+    }
+
+    // the scene record, built exactly as a handle builds it
+    SceneHost sc;
+    std::memset(sc.uni, 0, sizeof(sc.uni));
+    std::memcpy(sc.uni, uniforms, std::min(uniform_bytes, (size_t)MPM_UNIFORMS_BYTES));
+    if (collider_words) std::memcpy(sc.uni + 348, &num_indices, 4);  // GpuMpmPipelineManager.ts:80
+    sc.params = *params;
+    std::memset(&sc.dev, 0, sizeof(sc.dev));
+    sc.dev.col_data = collider_words ? collider_data : nullptr;
+    sc.dev.bvh = n_nodes ? (const uint32_t*)bvh_nodes : nullptr;
+    sc.dev.col_words = (uint32_t)collider_words;
+    sc.dev.n_nodes = n_nodes;
+    sc.dev.c_nidx = num_indices;
+    sc.dev.p_first = 0;
+    sc.dev.p_count = n_particles;
+    build_scene_dev(sc);
+    if (sc.dev.scale <= 0.0f || !(sc.dev.dt > 0.0f))
+        return na_fail(err, err_len, MPM_ERR_ARG, "fixedPointScale and timestep must be > 0");
+    if (sc.dev.res[0] <= 0 || sc.dev.res[1] <= 0 || sc.dev.res[2] <= 0)
+        return na_fail(err, err_len, MPM_ERR_ARG, "grid resolution must be > 0");
+    const uint32_t scene_first[2] = {0u, n_particles};
+
+    unsigned char* b = D.base;
+    Ctx c{};
+    c.particles = (float4*)particles;
+    c.order_in = (const uint32_t*)(b + NA_ORDER);
+    c.sorted = (uint32_t*)(b + NA_SORTED);
+    c.bin_slot = (uint32_t*)(b + NA_BIN_SLOT);
+    c.bin_rank = (uint32_t*)(b + NA_BIN_RANK);
+    c.keys = (unsigned long long*)(b + NA_KEYS);
+    c.slot_count = (uint32_t*)(b + NA_SLOT_COUNT);
+    c.slot_off = (uint32_t*)(b + NA_SLOT_OFF);
+    c.slot_st = (uint32_t*)(b + NA_SLOT_ST);
+    c.st_key = (unsigned long long*)(b + NA_ST_KEY);
+    c.st_slot = (uint32_t*)(b + NA_ST_SLOT);
+    c.st_begin = (uint32_t*)(b + NA_ST_BEGIN);
+    c.st_count = (uint32_t*)(b + NA_ST_COUNT);
+    c.chunk_nst = (uint32_t*)(b + NA_CHUNK_NST);
+    c.chunk_np = (uint32_t*)(b + NA_CHUNK_NP);
+    int4* tiles[2] = {(int4*)(b + NA_TILES0), (int4*)(b + NA_TILES1)};
+    c.tiles_a = tiles[0];
+    c.tiles_b = tiles[0];
+    c.scenes = (const SceneDev*)(b + NA_SCENE);
+    c.scene_first = (const uint32_t*)(b + NA_SCENE_FIRST);
+    c.counters = (Counters*)(b + NA_COUNTERS);
+    c.n_particles = n_particles;
+    c.n_scenes = 1;
+    c.cap = MPM_NOALLOC_HASH_SLOTS;
+    c.max_tiles = MPM_NOALLOC_MAX_TILES;
+
+    cudaStream_t s = (cudaStream_t)stream;
+#define NA_CK(expr)                                                                                  \
+    do {                                                                                             \
+        cudaError_t _e = (expr);                                                                     \
+        if (_e != cudaSuccess) return na_fail(err, err_len, MPM_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+    // The array keeps the previous call's contents: start from an empty tile
+    // table, zero counters and status, and the identity particle order.
+    NA_CK(cudaMemsetAsync(c.keys, 0xff, NA_H * 8, s));
+    NA_CK(cudaMemsetAsync(c.slot_count, 0, NA_H * 4, s));
+    NA_CK(cudaMemsetAsync(c.counters, 0, sizeof(Counters), s));
+    NA_CK(cudaMemcpyAsync((void*)c.scenes, &sc.dev, sizeof(SceneDev), cudaMemcpyHostToDevice, s));
+    NA_CK(cudaMemcpyAsync((void*)c.scene_first, scene_first, sizeof(scene_first), cudaMemcpyHostToDevice, s));
+    k_iota<<<(n_particles + 255u) / 256u, 256, 0, s>>>((uint32_t*)c.order_in, n_particles);
+    NA_CK(cudaGetLastError());
+    auto run = [&](uint32_t kid) {
+        int grid = std::max(1, D.n_sms * std::max(1, D.blocks_per_sm[kid]));
+        return launch_kernel<NA_EDGE>(kid, c, s, grid, 0, 0, nullptr);
+    };
+    for (uint32_t k : {K_BIN_INSERT, K_COMPACT_A, K_COMPACT_B, K_COMPACT_C, K_BIN_SCATTER}) NA_CK(run(k));
+    if (method == MPM_METHOD_EXPLICIT) {
+        NA_CK(run(K_P2G_EXPLICIT));
+        NA_CK(run(K_G2P_EXPLICIT));
+    } else {
+        int cur = 0;
+        c.tiles_a = tiles[cur];
+        NA_CK(run(K_PBMPM_FIRST));
+        for (uint32_t it = 1; it < params->n_iter; it++) {
+            c.tiles_b = tiles[cur];
+            c.tiles_a = tiles[cur ^ 1];
+            NA_CK(run(K_PBMPM_ITER));
+            cur ^= 1;
+        }
+        c.tiles_b = tiles[cur];
+        NA_CK(run(K_G2P_PBMPM));
+    }
+    if (status_out) {
+        Counters ct;
+        NA_CK(cudaMemcpyAsync(&ct, c.counters, sizeof(ct), cudaMemcpyDeviceToHost, s));
+        NA_CK(cudaStreamSynchronize(s));
+        *status_out = ct.status;
+        if (ct.status)
+            return na_fail(err, err_len, MPM_ERR_DEVICE_STATUS,
+                           "device status 0x%x (0x2: more than %u occupied tiles; 0x1: tile hash full)", ct.status,
+                           MPM_NOALLOC_MAX_TILES);
+    }
+#undef NA_CK
     return MPM_OK;
 }
