@@ -162,12 +162,14 @@ const char* mpm_kernel_name(uint32_t kernel_id);
 uint32_t mpm_kernel_count(void);
 /* Captures each substep into a CUDA graph (default on). */
 int mpm_use_graphs(MpmHandle* h, int enable);
-/* Device self-test of the step's arithmetic helpers: compares the
- * corrected-reciprocal division against IEEE division on n pseudo-random
- * operand pairs and checks the saturating f32->i32 conversion (bit mask of
- * failed cases).  Both must be 0.  nan_conversion reports the hardware's raw
- * truncating conversion of a NaN. */
-int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div_mismatches, uint64_t* cvt_mismatches,
+/* Device self-test of the step's arithmetic helpers, on n pseudo-random
+ * operand pairs: the folded fixed-point encoding i32(x * (r * 2^k)) against
+ * i32((x * r) * 2^k), and the device reciprocal against the IEEE quotient
+ * 1/d (ident_mismatches counts failures of either); and the saturating
+ * f32->i32 conversion (cvt_mismatches: bit mask of failed cases).  Both must
+ * be 0.  nan_conversion reports the hardware's raw truncating conversion of
+ * a NaN. */
+int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* ident_mismatches, uint64_t* cvt_mismatches,
                  uint64_t* nan_conversion);
 
 /* ---- allocation-free substep ----------------------------------------
@@ -204,7 +206,7 @@ int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div_mismatches
 #define MPM_NOALLOC_MAX_TILES 512u
 #define MPM_NOALLOC_TILE_EDGE 8u
 #define MPM_NOALLOC_HASH_SLOTS 8192u
-#define MPM_NOALLOC_SCRATCH_BYTES (18u << 20)
+#define MPM_NOALLOC_SCRATCH_BYTES (25u << 20)
 int mpm_step_noalloc(int device, void* stream, void* particles, uint32_t n_particles, int method,
                      const void* uniforms, size_t uniform_bytes, const MpmParams* params,
                      const uint32_t* collider_data, size_t collider_words, uint32_t num_indices,

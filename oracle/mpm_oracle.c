@@ -3,20 +3,30 @@
  * MPM step; see mpm_oracle.h for the scope and the parity status (UNPINNED).
  *
  * Compiled twice: -DOR_FP64=0 gives the orf_* (f32, fixed-point grid) symbols,
- * -DOR_FP64=1 the ord_* (f64) symbols.  Build with -ffp-contract=off and
- * without -ffast-math: the f32 instantiation defines, operation by operation,
- * the canonical evaluation order the CUDA path must reproduce bit for bit.
+ * -DOR_FP64=1 the ord_* (f64) symbols.  Build with -ffp-contract=off (every
+ * fused multiply-add is written out as fmaf) and without -ffast-math: the f32
+ * instantiation defines, operation by operation, the canonical evaluation
+ * order the CUDA path must reproduce bit for bit.
  *
- * Canonical evaluation rules (the WGSL leaves them to the implementation):
- *   dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z
- *   (M*v)[r] = (M[0][r]*v.x + M[1][r]*v.y) + M[2][r]*v.z   (column-major M[c][r])
- *   (A*B)[c][r] = (A[0][r]*B[c][0] + A[1][r]*B[c][1]) + A[2][r]*B[c][2]
- *   det(M) = (M00*(M11*M22 - M21*M12) - M10*(M01*M22 - M21*M02)) + M20*(M01*M12 - M11*M02)
- *            with Mcr = M[c][r]
- *   length(v) = sqrt(dot(v,v)); normalize(v) = v / length(v)
+ * Canonical evaluation rules.  WGSL leaves operation fusion and the exact
+ * rounding of division, exp and pow to the implementation (division is
+ * specified to 2.5 ulp); the oracle fixes one choice within those bounds:
+ *   fma(a,b,c) = a*b+c rounded once (C fmaf); M[c][r] is column-major
+ *   dot(a,b)     = fma(a.z, b.z, fma(a.y, b.y, a.x*b.x))
+ *   (M*v)[r]     = fma(M[2][r], v.z, fma(M[1][r], v.y, M[0][r]*v.x))
+ *   (A*B)[c][r]  = fma(A[2][r], B[c][2], fma(A[1][r], B[c][1], A[0][r]*B[c][0]))
+ *   cross(a,b).x = fma(a.y, b.z, -(a.z*b.y)), and cyclically
+ *   det(M)       = fma(M20, k2, fma(-M10, k1, M00*k0)), k0 = fma(M11, M22, -(M21*M12)),
+ *                  k1 = fma(M01, M22, -(M21*M02)), k2 = fma(M01, M12, -(M11*M02))
+ *   s += a*b     = fma(a, b, s) in the transfer sums (velocity, B, velocity gradient)
+ *   x / d for d constant over the substep (dt, cell size, fixed-point scale,
+ *                  force divisor) = x * RN(1/d), error <= 1.5 ulp
+ *   momentum / cell mass = momentum * RN(1/mass)
+ *   every other division, and sqrt, are IEEE; length(v) = sqrt(dot(v,v))
  *   i32(f) = truncation toward zero, saturating, NaN -> 0
  *   exp/pow evaluated in f64 by or_exp64/or_log64 below, rounded once to f32
- * Every other expression follows the WGSL source's own left-to-right order.
+ * Every other expression follows the WGSL source's own left-to-right order;
+ * the f64 instantiation uses the same formulas with IEEE f64 division.
  */
 #include "mpm_oracle.h"
 #include <math.h>
@@ -176,6 +186,9 @@ void or_default_ext(OrExt* e) {
 /* precision-dependent scalar ops                                      */
 /* ------------------------------------------------------------------ */
 #if OR_FP64
+#define FMA(a, b, c) fma((a), (b), (c))
+/* x / d for a divisor constant over the substep; rd = RN(1/d) in f32 */
+#define KDIV(x, d, rd) ((x) / (d))
 static inline real r_exp(real x) { return exp(x); }
 static inline real r_pow(real x, real y) { return pow(x, y); }
 static inline real r_sqrt(real x) { return sqrt(x); }
@@ -183,6 +196,8 @@ static inline real r_min(real a, real b) { return fmin(a, b); }
 static inline real r_max(real a, real b) { return fmax(a, b); }
 static inline real r_abs(real a) { return fabs(a); }
 #else
+#define FMA(a, b, c) fmaf((a), (b), (c))
+#define KDIV(x, d, rd) ((x) * (rd))
 static inline real r_exp(real x) { return (float)or_exp64((double)x); }
 static inline real r_pow(real x, real y) { return or_powf(x, y); }
 static inline real r_sqrt(real x) { return sqrtf(x); }
@@ -203,20 +218,20 @@ static inline real sgn(real x) { return x > 0 ? (real)1 : (x < 0 ? (real)-1 : (r
 /* ------------------------------------------------------------------ */
 /* vector / matrix helpers (matrixOps.wgsl; WGSL builtins)             */
 /* ------------------------------------------------------------------ */
-static inline real dot3(const real* a, const real* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+static inline real dot3(const real* a, const real* b) { return FMA(a[2], b[2], FMA(a[1], b[1], a[0] * b[0])); }
 static inline void cross3(const real* a, const real* b, real* o) {
-    real x = a[1] * b[2] - a[2] * b[1];
-    real y = a[2] * b[0] - a[0] * b[2];
-    real z = a[0] * b[1] - a[1] * b[0];
+    real x = FMA(a[1], b[2], -(a[2] * b[1]));
+    real y = FMA(a[2], b[0], -(a[0] * b[2]));
+    real z = FMA(a[0], b[1], -(a[1] * b[0]));
     o[0] = x; o[1] = y; o[2] = z;
 }
 static inline real len3(const real* a) { return r_sqrt(dot3(a, a)); }
 
 static inline real det3(const real* m) {
-    real t0 = m[0] * (m[4] * m[8] - m[7] * m[5]);
-    real t1 = m[3] * (m[1] * m[8] - m[7] * m[2]);
-    real t2 = m[6] * (m[1] * m[5] - m[4] * m[2]);
-    return (t0 - t1) + t2;
+    real k0 = FMA(m[4], m[8], -(m[7] * m[5]));
+    real k1 = FMA(m[1], m[8], -(m[7] * m[2]));
+    real k2 = FMA(m[1], m[5], -(m[4] * m[2]));
+    return FMA(m[6], k2, FMA(-m[3], k1, m[0] * k0));
 }
 
 static const real IDENT[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
@@ -226,15 +241,15 @@ static inline void inv3(const real* m, real* o) {
     real det = det3(m);
     if (det == 0) { memcpy(o, IDENT, sizeof(IDENT)); return; }
     real a[9];
-    a[0] = m[4] * m[8] - m[5] * m[7];
-    a[1] = m[2] * m[7] - m[1] * m[8];
-    a[2] = m[1] * m[5] - m[2] * m[4];
-    a[3] = m[5] * m[6] - m[3] * m[8];
-    a[4] = m[0] * m[8] - m[2] * m[6];
-    a[5] = m[2] * m[3] - m[0] * m[5];
-    a[6] = m[3] * m[7] - m[4] * m[6];
-    a[7] = m[1] * m[6] - m[0] * m[7];
-    a[8] = m[0] * m[4] - m[1] * m[3];
+    a[0] = FMA(m[4], m[8], -(m[5] * m[7]));
+    a[1] = FMA(m[2], m[7], -(m[1] * m[8]));
+    a[2] = FMA(m[1], m[5], -(m[2] * m[4]));
+    a[3] = FMA(m[5], m[6], -(m[3] * m[8]));
+    a[4] = FMA(m[0], m[8], -(m[2] * m[6]));
+    a[5] = FMA(m[2], m[3], -(m[0] * m[5]));
+    a[6] = FMA(m[3], m[7], -(m[4] * m[6]));
+    a[7] = FMA(m[1], m[6], -(m[0] * m[7]));
+    a[8] = FMA(m[0], m[4], -(m[1] * m[3]));
     real s = (real)1 / det;
     for (int i = 0; i < 9; i++) o[i] = a[i] * s;
 }
@@ -249,13 +264,13 @@ static inline void mul3(const real* A, const real* B, real* o) {
     real t[9];
     for (int c = 0; c < 3; c++)
         for (int r = 0; r < 3; r++)
-            t[c * 3 + r] = (A[0 * 3 + r] * B[c * 3 + 0] + A[1 * 3 + r] * B[c * 3 + 1]) + A[2 * 3 + r] * B[c * 3 + 2];
+            t[c * 3 + r] = FMA(A[2 * 3 + r], B[c * 3 + 2], FMA(A[1 * 3 + r], B[c * 3 + 1], A[0 * 3 + r] * B[c * 3 + 0]));
     memcpy(o, t, sizeof(t));
 }
 
 static inline void mv3(const real* M, const real* v, real* o) {
     real t[3];
-    for (int r = 0; r < 3; r++) t[r] = (M[0 * 3 + r] * v[0] + M[1 * 3 + r] * v[1]) + M[2 * 3 + r] * v[2];
+    for (int r = 0; r < 3; r++) t[r] = FMA(M[2 * 3 + r], v[2], FMA(M[1 * 3 + r], v[1], M[0 * 3 + r] * v[0]));
     o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
 }
 
@@ -276,7 +291,7 @@ static inline void polar3(const real* F, real* R) {
 static inline void xform_point(const real* M, const real* v, real* o) {
     real t[3];
     for (int r = 0; r < 3; r++)
-        t[r] = ((M[0 * 4 + r] * v[0] + M[1 * 4 + r] * v[1]) + M[2 * 4 + r] * v[2]) + M[3 * 4 + r] * (real)1;
+        t[r] = FMA(M[2 * 4 + r], v[2], FMA(M[1 * 4 + r], v[1], M[0 * 4 + r] * v[0])) + M[3 * 4 + r];
     o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
 }
 
@@ -299,6 +314,9 @@ typedef struct Scene {
     int32_t bc;
     uint32_t gaxis;
     real cmargin, csurf, cthr, cfric, cvs, blend, vexp;
+    /* RN(1/d) of the substep-constant divisors (f32 instantiation), and
+     * g*dt rounded once (gridUpdate.cs.wgsl:44) */
+    real rdt, rcd[3], rscale, rfdiv, gdt[3];
 } Scene;
 
 static inline float rdf(const uint8_t* u, size_t off) { float f; memcpy(&f, u + off, 4); return f; }
@@ -352,6 +370,11 @@ static void load_scene(Scene* s, const uint8_t* u, const OrExt* e) {
     s->cvs = e->collider_vel_scale;
     s->blend = e->pbmpm_blend;
     s->vexp = e->pbmpm_volume_exponent;
+    s->rdt = (real)1 / s->dt;
+    for (int i = 0; i < 3; i++) s->rcd[i] = (real)1 / s->cd[i];
+    s->rscale = (real)1 / s->scale;
+    s->rfdiv = (real)1 / s->fdiv;
+    for (int i = 0; i < 3; i++) s->gdt[i] = s->g[i] * s->dt;
 }
 
 /* ------------------------------------------------------------------ */
@@ -399,22 +422,22 @@ static inline void p_store(PART* p, const PS* s) {
 /* grid geometry (mpmOps.wgsl:14-53)                                    */
 /* ------------------------------------------------------------------ */
 static inline void cell_number(const Scene* s, const real* pos, int32_t* c) {
-    for (int i = 0; i < 3; i++) c[i] = to_i32((pos[i] - s->gmin[i]) / s->cd[i]);
+    for (int i = 0; i < 3; i++) c[i] = to_i32(KDIV(pos[i] - s->gmin[i], s->cd[i], s->rcd[i]));
 }
 static inline int in_range(const Scene* s, const int32_t* c) {
     return 0 <= c[0] && 0 <= c[1] && 0 <= c[2] && c[0] < s->res[0] && c[1] < s->res[1] && c[2] < s->res[2];
 }
 static inline void frac_pos(const Scene* s, const real* pos, const int32_t* c, real* f) {
     for (int i = 0; i < 3; i++) {
-        real mn = s->gmin[i] + s->cd[i] * (real)c[i];
-        f[i] = (pos[i] - mn) / s->cd[i];
+        real mn = FMA(s->cd[i], (real)c[i], s->gmin[i]);
+        f[i] = KDIV(pos[i] - mn, s->cd[i], s->rcd[i]);
     }
 }
 /* w[k][axis], k = offset + 1 */
 static inline void bspline_w(const real* f, real w[3][3]) {
     for (int i = 0; i < 3; i++) {
         w[0][i] = ((real)0.5 * ((real)1 - f[i])) * ((real)1 - f[i]);
-        w[1][i] = (real)0.75 - (f[i] - (real)0.5) * (f[i] - (real)0.5);
+        w[1][i] = FMA(-(f[i] - (real)0.5), f[i] - (real)0.5, (real)0.75);
         w[2][i] = ((real)0.5 * f[i]) * f[i];
     }
 }
@@ -593,7 +616,7 @@ static void stress_pk1(const Scene* s, const PS* p, real* P) {
     tr3(Fi, FiT);
     real a = (real)2 * mu;
     real b = (la * (J - (real)1)) * J;
-    for (int i = 0; i < 9; i++) P[i] = a * (p->Fe[i] - R[i]) + b * FiT[i];
+    for (int i = 0; i < 9; i++) P[i] = FMA(b, FiT[i], a * (p->Fe[i] - R[i]));
 }
 
 /* ------------------------------------------------------------------ */
@@ -622,13 +645,13 @@ static void p2g_explicit(OrCtx* c, const Scene* s, const PS* p) {
                 if (ci == EMPTY_IDX) continue;
                 real wgt = (w[ox + 1][0] * w[oy + 1][1]) * w[oz + 1][2];
                 real g[3];
-                g[0] = ((dw[ox + 1][0] * w[oy + 1][1]) * w[oz + 1][2]) / s->cd[0];
-                g[1] = ((w[ox + 1][0] * dw[oy + 1][1]) * w[oz + 1][2]) / s->cd[1];
-                g[2] = ((w[ox + 1][0] * w[oy + 1][1]) * dw[oz + 1][2]) / s->cd[2];
+                g[0] = KDIV((dw[ox + 1][0] * w[oy + 1][1]) * w[oz + 1][2], s->cd[0], s->rcd[0]);
+                g[1] = KDIV((w[ox + 1][0] * dw[oy + 1][1]) * w[oz + 1][2], s->cd[1], s->rcd[1]);
+                g[2] = KDIV((w[ox + 1][0] * w[oy + 1][1]) * dw[oz + 1][2], s->cd[2], s->rcd[2]);
                 real sf[3];
                 mv3(M, g, sf);
                 real mom[3];
-                for (int k = 0; k < 3; k++) mom[k] = wgt * pm[k] + sf[k] * s->dt;
+                for (int k = 0; k < 3; k++) mom[k] = FMA(wgt, pm[k], sf[k] * s->dt);
                 grid_add(c, ci, 1, ENC(mom[0], s->scale));
                 grid_add(c, ci, 2, ENC(mom[1], s->scale));
                 grid_add(c, ci, 3, ENC(mom[2], s->scale));
@@ -648,16 +671,16 @@ static void pbmpm_constraints(const Scene* s, PS* p) {
     real ob = (real)1 - s->blend;
     for (int i = 0; i < 9; i++) {
         real ts = Rt[i] * vs;
-        tb[i] = s->blend * ts + ob * Rt[i];
+        tb[i] = FMA(s->blend, ts, ob * Rt[i]);
     }
     inv3(p->Fe, Fei);
     mul3(tb, Fei, Dc);
     for (int i = 0; i < 9; i++) Dc[i] = Dc[i] - IDENT[i];
     real J = det3(p->Fp);
-    real relax = (real)0.5 + (real)0.5 * ((real)1 - r_exp((-s->xi_p) / J));
+    real relax = FMA((real)0.5, (real)1 - r_exp((-s->xi_p) / J), (real)0.5);
     for (int i = 0; i < 9; i++) {
         real diff = Dc[i] - p->D[i];
-        p->D[i] = p->D[i] + relax * diff;
+        p->D[i] = FMA(relax, diff, p->D[i]);
     }
 }
 
@@ -683,7 +706,7 @@ static void p2g_pbmpm(OrCtx* c, const Scene* s, const PS* p, int with_forces) {
                 real off[3], aff[3], mom[3];
                 for (int k = 0; k < 3; k++) off[k] = (real)cc[k] - pcp[k];
                 mv3(p->D, off, aff);
-                for (int k = 0; k < 3; k++) mom[k] = (wm * (p->dxp[k] + aff[k])) / s->dt;
+                for (int k = 0; k < 3; k++) mom[k] = KDIV(wm * (p->dxp[k] + aff[k]), s->dt, s->rdt);
                 grid_add(c, ci, 1, ENC(mom[0], s->scale));
                 grid_add(c, ci, 2, ENC(mom[1], s->scale));
                 grid_add(c, ci, 3, ENC(mom[2], s->scale));
@@ -723,7 +746,7 @@ static void p2g_pbmpm(OrCtx* c, const Scene* s, const PS* p, int with_forces) {
                         for (int k = 0; k < 3; k++) fo[k] = fo[k] + af[k];
                     }
                 }
-                for (int k = 0; k < 3; k++) fo[k] = fo[k] / s->fdiv;
+                for (int k = 0; k < 3; k++) fo[k] = KDIV(fo[k], s->fdiv, s->rfdiv);
                 real mc[3];
                 for (int k = 0; k < 3; k++) mc[k] = (fo[k] * wm) * s->dt;
                 grid_add(c, ci, 1, ENC(mc[0], s->scale));
@@ -740,12 +763,22 @@ static inline real cell_mass(const OrCtx* c, const Scene* s, uint32_t ci) { (voi
 static inline real cell_mom(const OrCtx* c, const Scene* s, uint32_t ci, int k) { (void)s; return c->grid[(size_t)ci * 4 + 1 + k]; }
 #else
 static inline real cell_mass(const OrCtx* c, const Scene* s, uint32_t ci) {
-    return (real)(int32_t)c->grid[(size_t)ci * 4] / s->scale;
+    return KDIV((real)(int32_t)c->grid[(size_t)ci * 4], s->scale, s->rscale);
 }
 static inline real cell_mom(const OrCtx* c, const Scene* s, uint32_t ci, int k) {
-    return (real)(int32_t)c->grid[(size_t)ci * 4 + 1 + k] / s->scale;
+    return KDIV((real)(int32_t)c->grid[(size_t)ci * 4 + 1 + k], s->scale, s->rscale);
 }
 #endif
+
+/* momentum / cell mass: momentum * RN(1/mass) in f32, IEEE division in f64 */
+static inline void div_mass(real* v, real m) {
+#if OR_FP64
+    for (int k = 0; k < 3; k++) v[k] = v[k] / m;
+#else
+    real rm = (real)1 / m;
+    for (int k = 0; k < 3; k++) v[k] = v[k] * rm;
+#endif
+}
 
 /* Grid-side boundary of boundary_mode 1 (an extension: sticky ground plane at
  * the grid minimum of `ground_axis`, slip walls elsewhere). */
@@ -770,8 +803,9 @@ static void grid_update_explicit(OrCtx* c, const Scene* s) {
             real m = cell_mass(c, s, ci);
             if (m <= 0) continue;
             real v[3];
-            for (int k = 0; k < 3; k++) v[k] = cell_mom(c, s, ci, k) / m;
-            for (int k = 0; k < 3; k++) v[k] = v[k] + s->g[k] * s->dt;
+            for (int k = 0; k < 3; k++) v[k] = cell_mom(c, s, ci, k);
+            div_mass(v, m);
+            for (int k = 0; k < 3; k++) v[k] = v[k] + s->gdt[k];
             int32_t cc[3] = {bn[0] * 4 + (int32_t)(l & 3), bn[1] * 4 + (int32_t)((l >> 2) & 3), bn[2] * 4 + (int32_t)(l >> 4)};
             grid_bc(s, cc, v);
 #if OR_FP64
@@ -791,7 +825,7 @@ static inline int cell_velocity(const OrCtx* c, const Scene* s, const int32_t* c
     real m = cell_mass(c, s, ci);
     if (m <= 0) return 0;
     for (int k = 0; k < 3; k++) v[k] = cell_mom(c, s, ci, k);
-    for (int k = 0; k < 3; k++) v[k] = v[k] / m;
+    div_mass(v, m);
     if (pbmpm) grid_bc(s, cc, v);
     return 1;
 }
@@ -816,20 +850,20 @@ static void g2p(const OrCtx* c, const Scene* s, PS* p, int pbmpm) {
                 if (!cell_velocity(c, s, cc, pbmpm, cv)) continue;
                 real wgt = (w[ox + 1][0] * w[oy + 1][1]) * w[oz + 1][2];
                 if (!pbmpm) {
-                    for (int k = 0; k < 3; k++) nv[k] = nv[k] + wgt * cv[k];
+                    for (int k = 0; k < 3; k++) nv[k] = FMA(wgt, cv[k], nv[k]);
                     real g[3];
                     g[0] = (dw[ox + 1][0] * w[oy + 1][1]) * w[oz + 1][2];
                     g[1] = (w[ox + 1][0] * dw[oy + 1][1]) * w[oz + 1][2];
                     g[2] = (w[ox + 1][0] * w[oy + 1][1]) * dw[oz + 1][2];
                     for (int col = 0; col < 3; col++)
-                        for (int r = 0; r < 3; r++) G[col * 3 + r] = G[col * 3 + r] + g[col] * cv[r];
+                        for (int r = 0; r < 3; r++) G[col * 3 + r] = FMA(g[col], cv[r], G[col * 3 + r]);
                 } else {
-                    for (int k = 0; k < 3; k++) nv[k] = nv[k] + wgt * cv[k];
+                    for (int k = 0; k < 3; k++) nv[k] = FMA(wgt, cv[k], nv[k]);
                     real wv[3] = {wgt * cv[0], wgt * cv[1], wgt * cv[2]};
                     real dist[3];
                     for (int k = 0; k < 3; k++) dist[k] = (real)cc[k] - pcp[k];
                     for (int col = 0; col < 3; col++)
-                        for (int r = 0; r < 3; r++) G[col * 3 + r] = G[col * 3 + r] + wv[r] * dist[col];
+                        for (int r = 0; r < 3; r++) G[col * 3 + r] = FMA(wv[r], dist[col], G[col * 3 + r]);
                 }
             }
     for (int k = 0; k < 3; k++) p->vel[k] = nv[k];
@@ -1036,12 +1070,12 @@ static void collide(OrCtx* ctx, const Scene* s, const OrCollider* col, PS* p) {
             }
         }
     }
-    real vsf = s->cvs / s->dt;
+    real vsf = KDIV(s->cvs, s->dt, s->rdt);
     if (has_hit) {
         real sm = s->csurf;
         real ov[3], vr[3], vn, vt[3], nvv[3];
         for (int k = 0; k < 3; k++) p->pos[k] = hpos[k] + hnorm[k] * sm;
-        for (int k = 0; k < 3; k++) ov[k] = p->dxp[k] / s->dt;
+        for (int k = 0; k < 3; k++) ov[k] = KDIV(p->dxp[k], s->dt, s->rdt);
         for (int k = 0; k < 3; k++) vr[k] = ov[k] - s->cvel[k];
         vn = dot3(vr, hnorm);
         for (int k = 0; k < 3; k++) vt[k] = vr[k] - vn * hnorm[k];
@@ -1062,7 +1096,7 @@ static void collide(OrCtx* ctx, const Scene* s, const OrCollider* col, PS* p) {
         for (int k = 0; k < 3; k++) pd[k] = df[k] / ld;
     if (dist < s->cthr) {
         real ov[3], vr[3], vn, vt[3], nvv[3];
-        for (int k = 0; k < 3; k++) ov[k] = p->dxp[k] / s->dt;
+        for (int k = 0; k < 3; k++) ov[k] = KDIV(p->dxp[k], s->dt, s->rdt);
         for (int k = 0; k < 3; k++) vr[k] = ov[k] - s->cvel[k];
         vn = dot3(vr, pd);
         for (int k = 0; k < 3; k++) vt[k] = vr[k] - vn * pd[k];

@@ -2,7 +2,8 @@
 
 Bar: the fixed-point grid is compared bit for bit, and so are the particle
 fields, because the CUDA path evaluates the oracle's canonical operation
-order (no FMA contraction, IEEE division, the same f64 exp/log).  Where a
+order (the same fused multiply-adds, reciprocal products for substep-constant
+divisors, the same f64 exp/log).  Where a
 test states a tolerance it is the relative bound 1e-5 on single-step fields.
 """
 import numpy as np
@@ -14,12 +15,13 @@ pytestmark = pytest.mark.gpu
 
 
 def test_device_arithmetic_selftest(gpu):
-    """The corrected-reciprocal division equals IEEE division bit for bit on
-    2^28 random operand pairs, and f32->i32 saturates with NaN -> 0."""
+    """On 2^28 random operand pairs the folded fixed-point encoding equals the
+    two-product one after i32 conversion and the device reciprocal equals the
+    IEEE quotient 1/d; f32->i32 saturates with NaN -> 0."""
     import ctypes as C
     a, b, nanv = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
     assert gpu.load().mpm_selftest(0, 1 << 28, 12345, C.byref(a), C.byref(b), C.byref(nanv)) == 0
-    assert a.value == 0, f"{a.value} division mismatches"
+    assert a.value == 0, f"{a.value} identity mismatches"
     assert b.value == 0, f"conversion mismatch code {b.value}"
 
 
@@ -69,6 +71,19 @@ def test_multi_step_bit_exact_and_aggregates(gpu, oracle_mod, kind):
     c32 = oracle_mod.aggregates(got["pos"], got["vel"], got["mass"], got["Fp"][:, :, :3].reshape(-1, 9))
     c64 = oracle_mod.aggregates(w64["pos"], w64["vel"], w64["mass"], w64["Fp"])
     assert np.allclose(c32[0], c64[0], rtol=1e-3, atol=1e-3)
+    g.close()
+
+
+@pytest.mark.parametrize("kind,interaction", [("explicit", False), ("pbmpm", True)])
+def test_non_power_of_two_scale_bit_exact(gpu, oracle_mod, kind, interaction):
+    """A fixed-point scale that is not a power of two takes the unfolded
+    encoding i32((x * RN(1/dt)) * scale); it matches the oracle as well."""
+    spec = _scene(gpu, kind=kind, with_collider=True, interaction=interaction)
+    spec.uniforms.write_fixed_point_scale(3.0 * 2.0 ** 26)
+    g = GpuScene(gpu, spec)
+    assert g.step(2) == 0
+    _, want = run_oracle(oracle_mod, spec, n_steps=2)
+    compare_states(g.particles(), want)
     g.close()
 
 

@@ -80,6 +80,7 @@ struct MpmHandle {
     uint32_t* chunk_nst = nullptr;
     uint32_t* chunk_np = nullptr;
     int4* tiles[2] = {nullptr, nullptr};
+    float4* iter_rec = nullptr;   // PBMPM iteration records, IR_PLANES x N float4
     int last_tiles = 0;
     SceneDev* d_scenes = nullptr;
     uint32_t* d_scene_first = nullptr;
@@ -233,36 +234,37 @@ static void build_scene_dev(SceneHost& s) {
     d.bvh = bvh;
     d.col_words = col_words;
     d.n_nodes = n_nodes;
-    // Reciprocals of the constant divisors, rounded once in f32 (an IEEE
-    // single division on the host), and the exact division mode each allows.
-    auto mode = [](float v, bool int_valued) -> uint32_t {
-        uint32_t b;
-        std::memcpy(&b, &v, 4);
-        int ex = (int)((b >> 23) & 0xff) - 127;
-        bool pow2 = (b & 0x807fffffu) == 0u && ex > -127 && ex < 128;
-        if (pow2 && ex <= 0) return DIV_POW2;
-        if (pow2 && int_valued && ex <= 100) return DIV_POW2S;
-        float a = std::fabs(v);
-        return (a >= 0x1p-40f && a <= 0x1p40f) ? DIV_CORR : DIV_IEEE;
+    // Reciprocals RN(1/d) of the substep-constant divisors: one IEEE single
+    // division each on the host, the value the oracle forms the same way.
+    auto recip = [](float v) {
+        volatile float one = 1.0f;
+        return v != 0.0f ? one / v : 0.0f;
     };
-    auto recip = [](float v) { return v != 0.0f ? 1.0f / v : 0.0f; };
-    d.mdt = mode(d.dt, false);
     d.rdt = recip(d.dt);
-    for (int i = 0; i < 3; i++) {
-        d.mcd[i] = mode(d.cd[i], false);
-        d.rcd[i] = recip(d.cd[i]);
-    }
-    d.mscale = mode(d.scale, true);
+    for (int i = 0; i < 3; i++) d.rcd[i] = recip(d.cd[i]);
     d.rscale = recip(d.scale);
-    d.mfdiv = mode(d.fdiv, false);
     d.rfdiv = recip(d.fdiv);
     // loop-invariant operands of the step, each one IEEE f32 operation
-    // exactly as the kernels would compute it: g / force_divisor
+    // exactly as the kernels would compute it: g * RN(1/force_divisor)
     // (pbmpm.wgsl:137) and g * dt (gridUpdate.cs.wgsl:44)
     for (int i = 0; i < 3; i++) {
         volatile float gi = d.g[i];
-        d.gdiv[i] = gi / d.fdiv;
+        d.gdiv[i] = gi * d.rfdiv;
         d.gdt[i] = gi * d.dt;
+    }
+    // Folded encodings (SceneDev::fold): the scale must be 2^k, 0 <= k < 126,
+    // and RN(1/dt) * 2^k, dt * 2^k finite normal numbers (then exact).
+    {
+        uint32_t b;
+        std::memcpy(&b, &d.scale, 4);
+        int ex = (int)((b >> 23) & 0xffu) - 127;
+        bool pow2 = (b & 0x807fffffu) == 0u && ex >= 0 && ex < 126;
+        volatile float rdts = d.rdt * d.scale, dts = d.dt * d.scale;
+        bool ok = pow2 && std::isnormal((float)rdts) && std::isnormal((float)dts) && std::isnormal(d.rdt) &&
+                  std::isnormal(d.dt);
+        d.fold = ok ? 1u : 0u;
+        d.rdts = ok ? (float)rdts : 0.0f;
+        d.dts = ok ? (float)dts : 0.0f;
     }
 }
 
@@ -284,7 +286,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     for (auto e : h->event_pool) cudaEventDestroy(e);
     void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
-                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters};
+                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters, h->iter_rec};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h->own_particles && h->particles) cudaFree(h->particles);
@@ -373,6 +375,7 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     CK(h, cudaMalloc(&h->order[1], (size_t)N * 4));
     CK(h, cudaMalloc(&h->bin_slot, (size_t)N * 4));
     CK(h, cudaMalloc(&h->bin_rank, (size_t)N * 4));
+    CK(h, cudaMalloc(&h->iter_rec, (size_t)N * IR_PLANES * sizeof(float4)));
     CK(h, cudaMalloc(&h->d_scenes, (size_t)max_scenes * sizeof(SceneDev)));
     CK(h, cudaMalloc(&h->d_scene_first, (size_t)(max_scenes + 1) * 4));
     CK(h, cudaMalloc(&h->counters, sizeof(Counters)));
@@ -595,6 +598,7 @@ static Ctx make_ctx(MpmHandle* h, int parity) {
     c.chunk_np = h->chunk_np;
     c.tiles_a = h->tiles[0];
     c.tiles_b = h->tiles[0];
+    c.iter_rec = h->iter_rec;
     c.scenes = h->d_scenes;
     c.scene_first = h->d_scene_first;
     c.counters = h->counters;
@@ -850,7 +854,7 @@ extern "C" int mpm_sync(MpmHandle* h, uint32_t* status_out) {
     return MPM_OK;
 }
 
-extern "C" int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div_mismatches, uint64_t* cvt_mismatches,
+extern "C" int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* ident_mismatches, uint64_t* cvt_mismatches,
                             uint64_t* nan_conversion) {
     if (cudaSetDevice(device) != cudaSuccess) return MPM_ERR_CUDA;
     unsigned long long* d = nullptr;
@@ -862,7 +866,7 @@ extern "C" int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* div
     if (e == cudaSuccess) e = cudaMemcpy(hcnt, d, 24, cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) return MPM_ERR_CUDA;
-    if (div_mismatches) *div_mismatches = hcnt[0];
+    if (ident_mismatches) *ident_mismatches = hcnt[0];
     if (cvt_mismatches) *cvt_mismatches = hcnt[1];
     if (nan_conversion) *nan_conversion = hcnt[2];
     return MPM_OK;
@@ -971,7 +975,8 @@ constexpr size_t NA_CHUNK_NST = NA_ST_COUNT + na_round(NA_H * 4);
 constexpr size_t NA_CHUNK_NP = NA_CHUNK_NST + na_round(NA_H / COMPACT_CHUNK * 4);
 constexpr size_t NA_TILES0 = NA_CHUNK_NP + na_round(NA_H / COMPACT_CHUNK * 4);  // halo sums, int4
 constexpr size_t NA_TILES1 = NA_TILES0 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
-constexpr size_t NA_SCENE = NA_TILES1 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
+constexpr size_t NA_ITER_REC = NA_TILES1 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);  // PBMPM records
+constexpr size_t NA_SCENE = NA_ITER_REC + na_round(NA_P * IR_PLANES * 16);
 constexpr size_t NA_SCENE_FIRST = NA_SCENE + na_round(sizeof(SceneDev));
 constexpr size_t NA_COUNTERS = NA_SCENE_FIRST + na_round(2 * 4);
 constexpr size_t NA_BYTES = NA_COUNTERS + na_round(sizeof(Counters));
@@ -1098,6 +1103,7 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     int4* tiles[2] = {(int4*)(b + NA_TILES0), (int4*)(b + NA_TILES1)};
     c.tiles_a = tiles[0];
     c.tiles_b = tiles[0];
+    c.iter_rec = (float4*)(b + NA_ITER_REC);
     c.scenes = (const SceneDev*)(b + NA_SCENE);
     c.scene_first = (const uint32_t*)(b + NA_SCENE_FIRST);
     c.counters = (Counters*)(b + NA_COUNTERS);

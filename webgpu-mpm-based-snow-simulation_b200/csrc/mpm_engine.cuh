@@ -13,6 +13,7 @@
 //   st_key/st_slot/st_begin/st_count   per compact tile
 //   tiles[2]    max_tiles x (E+2)^3 x int4   per-tile halo sums
 //               (mass, momentum x, y, z) in the reference i32 fixed point
+//   iter_rec    IR_PLANES x N float4         PBMPM iteration records (below)
 //
 // A tile is E^3 grid cells (E = 8, 12 or 16, i.e. 2^3, 3^3 or 4^3 of the reference's
 // 4^3-cell blocks).  Its P2G writes the (E+2)^3 halo region it touches; the
@@ -30,6 +31,14 @@ constexpr uint32_t INVALID = 0xFFFFFFFFu;
 constexpr uint32_t MAX_PROBES = 1024u;
 constexpr int COMPACT_CHUNK = 4096;   // hash slots per compaction block (256 threads x 16)
 constexpr int KEY_BIAS = 32768;
+// PBMPM iteration record of one binned particle, stored plane by plane
+// (plane q of sorted position t at iter_rec[q * n + t]):
+//   0: pos.xyz, mass   1: Fe[0..3]   2: Fe[4..7]   3: Fe[8], Fe^-1[0..2]
+//   4: Fe^-1[3..6]     5: Fe^-1[7..8], elasticity relaxation, 0
+// Fe, Fp and the position do not change between the iterations of one
+// substep, so Fe^-1 and the relaxation factor (pbmpm.wgsl:29-35) are formed
+// once, by the first iteration, instead of once per iteration.
+constexpr int IR_PLANES = 6;
 
 // status bits (mirror of MPM_STATUS_* in include/mpm.h)
 constexpr uint32_t ST_HASH_FULL = 0x1u;
@@ -63,12 +72,18 @@ struct SceneDev {
     uint32_t col_words, n_nodes;
     const uint32_t* col_data;
     const uint32_t* bvh;
-    // host-rounded reciprocals RN(1/d) of the constant divisors and the
-    // division mode (DivMode) each may use
+    // reciprocals RN(1/d) of the substep-constant divisors, rounded once on
+    // the host: x / d evaluates as x * RN(1/d)
     float rdt, rcd[3], rscale, rfdiv;
-    float gdiv[3];     // gravity / force_divisor (pbmpm.wgsl:137), exact f32 quotient
-    float gdt[3];      // gravity * dt (gridUpdate.cs.wgsl:44), exact f32 product
-    uint32_t mdt, mcd[3], mscale, mfdiv;
+    float gdiv[3];     // gravity * RN(1/force_divisor) (pbmpm.wgsl:137)
+    float gdt[3];      // gravity * dt (gridUpdate.cs.wgsl:44)
+    // fixed-point encodings i32((x * RN(1/dt)) * scale) and
+    // i32(((f * wm) * dt) * scale): when scale = 2^k, 0 <= k < 126, scaling
+    // by it is exact for every value that can reach a nonzero i32, so the
+    // two products fold into one multiply by rdts = RN(1/dt) * 2^k or
+    // dts = dt * 2^k with the same i32 result
+    uint32_t fold;
+    float rdts, dts;
 };
 static_assert(sizeof(SceneDev) % 8 == 0, "SceneDev must be 8-byte sized");
 
@@ -97,6 +112,7 @@ struct Ctx {
     uint32_t* chunk_np;
     int4* tiles_a;            // tiles written by this pass's P2G
     int4* tiles_b;            // tiles read by this pass's G2P
+    float4* iter_rec;         // PBMPM iteration records, IR_PLANES x n float4, sorted order
     const SceneDev* scenes;
     const uint32_t* scene_first;  // n_scenes + 1 particle offsets
     Counters* counters;

@@ -82,22 +82,8 @@ __device__ __forceinline__ void load_scene_smem(SceneDev& dst, const SceneDev* s
     for (int i = threadIdx.x; i < (int)(sizeof(SceneDev) / 4); i += blockDim.x) d[i] = s[i];
 }
 
-__device__ __forceinline__ float inv_s(const SceneDev& S, int32_t v) {
-    // f32(i) / fixedPointScale
-    return divm(i2f(v), S.scale, S.rscale, S.mscale);
-}
-
-// x / m for the three momentum components of one cell: one reciprocal, then
-// the corrected division (bit-identical to x / m) while m is in range.
-struct CellDiv {
-    float m, r;
-    bool fast;
-    __device__ __forceinline__ explicit CellDiv(float mass) : m(mass) {
-        fast = mass >= 0x1p-40f && mass <= 0x1p40f;
-        r = fast ? __frcp_rn(mass) : 0.0f;
-    }
-    __device__ __forceinline__ float operator()(float x) const { return fast ? divc(x, m, r) : __fdiv_rn(x, m); }
-};
+// f32(i) / fixedPointScale
+__device__ __forceinline__ float inv_s(const SceneDev& S, int32_t v) { return fm(i2f(v), S.rscale); }
 
 // Grid-side boundary of boundary_mode 1 (an extension; the reference only
 // reflects particles): sticky ground plane, slip walls.
@@ -170,21 +156,18 @@ struct Stencil {
     float w[3][3];   // w[k][axis], k = offset + 1
 };
 
-__device__ __forceinline__ float div_cd(const SceneDev& S, float x, int i) { return divm(x, S.cd[i], S.rcd[i], S.mcd[i]); }
-__device__ __forceinline__ float div_dt(const SceneDev& S, float x) { return divm(x, S.dt, S.rdt, S.mdt); }
-
 __device__ __forceinline__ void make_stencil(const SceneDev& S, const float* pos, Stencil& st) {
 #pragma unroll
-    for (int i = 0; i < 3; i++) st.cell[i] = f2i(div_cd(S, fs(pos[i], S.gmin[i]), i));
+    for (int i = 0; i < 3; i++) st.cell[i] = f2i(fm(fs(pos[i], S.gmin[i]), S.rcd[i]));
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        float mn = fa(S.gmin[i], fm(S.cd[i], i2f(st.cell[i])));
-        float f = div_cd(S, fs(pos[i], mn), i);
+        float mn = ff(S.cd[i], i2f(st.cell[i]), S.gmin[i]);
+        float f = fm(fs(pos[i], mn), S.rcd[i]);
         st.f[i] = f;
         float om = fs(1.0f, f);
         st.w[0][i] = fm(fm(0.5f, om), om);
         float h = fs(f, 0.5f);
-        st.w[1][i] = fs(0.75f, fm(h, h));
+        st.w[1][i] = ff(-h, h, 0.75f);
         st.w[2][i] = fm(fm(0.5f, f), f);
     }
 }
@@ -218,13 +201,21 @@ __device__ __forceinline__ void stress_matrix(const SceneDev& S, const PState& p
     for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int r = 0; r < 3; r++) {
-            float Prc = fa(fm(a, fs(p.Fe[r * 3 + c], R[r * 3 + c])), fm(b, Fi[c * 3 + r]));
+            float Prc = ff(b, Fi[c * 3 + r], fm(a, fs(p.Fe[r * 3 + c], R[r * 3 + c])));
             M[c * 3 + r] = fm(nV, Prc);
         }
 }
 
-// solveParticleConstraints (pbmpm.wgsl:16-39): updates D.
-__device__ __forceinline__ void pbmpm_constraints(const SceneDev& S, const float* Fe, const float* Fp, float* D) {
+// elasticity relaxation factor 0.5 + 0.5 (1 - exp(-xi / det Fp)) (pbmpm.wgsl:29-35)
+__device__ __forceinline__ float pbmpm_relax(const SceneDev& S, const float* Fp) {
+    float J = det3(Fp);
+    return ff(0.5f, fs(1.0f, expf_m(fd(-S.xi_p, J))), 0.5f);
+}
+
+// solveParticleConstraints (pbmpm.wgsl:16-39): updates D, given Fe, its
+// inverse and the relaxation factor (both fixed within a substep).
+__device__ __forceinline__ void pbmpm_constraints(const SceneDev& S, const float* Fe, const float* Fei, float relax,
+                                                  float* D) {
     float IpD[9], Ft[9], Rt[9];
 #pragma unroll
     for (int i = 0; i < 9; i++) IpD[i] = fa((i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f, D[i]);
@@ -233,17 +224,14 @@ __device__ __forceinline__ void pbmpm_constraints(const SceneDev& S, const float
     float tv = det3(Ft);
     float vs = powf_m(fabsf(tv), S.vexp);
     float ob = fs(1.0f, S.blend);
-    float tb[9], Fei[9], Dc[9];
+    float tb[9], Dc[9];
 #pragma unroll
-    for (int i = 0; i < 9; i++) tb[i] = fa(fm(S.blend, fm(Rt[i], vs)), fm(ob, Rt[i]));
-    inv3(Fe, Fei);
+    for (int i = 0; i < 9; i++) tb[i] = ff(S.blend, fm(Rt[i], vs), fm(ob, Rt[i]));
     mul3(tb, Fei, Dc);
-    float J = det3(Fp);
-    float relax = fa(0.5f, fm(0.5f, fs(1.0f, expf_m(fd(-S.xi_p, J)))));
 #pragma unroll
     for (int i = 0; i < 9; i++) {
         float dci = fs(Dc[i], (i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f);
-        D[i] = fa(D[i], fm(relax, fs(dci, D[i])));
+        D[i] = ff(relax, fs(dci, D[i]), D[i]);
     }
 }
 
@@ -449,13 +437,13 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
             }
         }
     }
-    float vsf = fd(S.cvs, S.dt);
+    float vsf = fm(S.cvs, S.rdt);
     if (has_hit) {
         float nvv[3], vr[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) p.pos[k] = fa(hpos[k], fm(hnorm[k], S.csurf));
 #pragma unroll
-        for (int k = 0; k < 3; k++) vr[k] = fs(div_dt(S, p.dxp[k]), S.cvel[k]);
+        for (int k = 0; k < 3; k++) vr[k] = fs(fm(p.dxp[k], S.rdt), S.cvel[k]);
         float vn = dot3(vr, hnorm);
         float om = fs(1.0f, S.cfric);
 #pragma unroll
@@ -479,7 +467,7 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
     if (dist < S.cthr) {
         float nvv[3], vr[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) vr[k] = fs(div_dt(S, p.dxp[k]), S.cvel[k]);
+        for (int k = 0; k < 3; k++) vr[k] = fs(fm(p.dxp[k], S.rdt), S.cvel[k]);
         float vn = dot3(vr, pd);
         float om = fs(1.0f, 0.0f);
 #pragma unroll
@@ -540,7 +528,7 @@ __global__ void __launch_bounds__(256) k_bin_insert(Ctx c) {
         float pos[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            int cell = f2i(fd(fs(pos[i], __ldg(&S->gmin[i])), __ldg(&S->cd[i])));
+            int cell = f2i(fm(fs(pos[i], __ldg(&S->gmin[i])), __ldg(&S->rcd[i])));
             int res = __ldg(&S->res[i]);
             // cells below -1 or above res reach no grid cell; clamping them
             // only decides which tile processes the particle
@@ -767,19 +755,19 @@ __device__ __forceinline__ float4 cell_velocity(const SceneDev& S, int4 s, const
     bool in = gc[0] >= 0 && gc[1] >= 0 && gc[2] >= 0 && gc[0] < S.res[0] && gc[1] < S.res[1] && gc[2] < S.res[2];
     float cm = inv_s(S, s.x);
     if (!in || cm <= 0.0f) return make_float4(0.f, 0.f, 0.f, 0.f);
-    CellDiv dm(cm);
+    float rm = __frcp_rn(cm);
     int32_t mi[3] = {s.y, s.z, s.w};
     if (!PB) {
         float u[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) u[k] = fa(dm(inv_s(S, mi[k])), S.gdt[k]);
+        for (int k = 0; k < 3; k++) u[k] = fa(fm(inv_s(S, mi[k]), rm), S.gdt[k]);
         grid_bc(S, gc, u);
 #pragma unroll
         for (int k = 0; k < 3; k++) mi[k] = f2i(fm(fm(u[k], cm), S.scale));
     }
     float v[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) v[k] = dm(inv_s(S, mi[k]));
+    for (int k = 0; k < 3; k++) v[k] = fm(inv_s(S, mi[k]), rm);
     if (PB) grid_bc(S, gc, v);
     return make_float4(v[0], v[1], v[2], 0.f);
 }
@@ -902,11 +890,13 @@ __device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const 
 }
 
 // G2P gather from the shared velocity tile (gridToParticle.cs.wgsl:28-130).
-// Cells the reference skips hold velocity 0 here; adding w*0 (+0 or -0) to a
-// running sum that starts at +0 leaves it unchanged, so the sums are equal.
+// Cells the reference skips hold velocity 0 here: each of their terms is a
+// product with a zero factor, and adding +-0 to a sum that started at +0
+// leaves it unchanged, so the sums are equal.  The summation order is the
+// reference's loop order (z outermost, x innermost).
 template <int E, bool PB>
-__device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& T, const float4* vel,
-                                           const Stencil& sc, float* nv, float* G) {
+__device__ __forceinline__ void g2p_gather(const TileCtx<E>& T, const float4* vel, const Stencil& sc, float* nv,
+                                           float* G) {
     constexpr int H = E + 2;
 #pragma unroll
     for (int k = 0; k < 3; k++) nv[k] = 0.f;
@@ -920,7 +910,7 @@ __device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& 
         inside = inside && l0[k] >= 0 && l0[k] < E;
     }
     if (!inside) return;
-    float offs[3][3];  // offs[axis][o] = (cell + o - 1) - particle_cell_pos, formed once per axis
+    float offs[3][3];  // offs[axis][o] = (cell + o - 1) - particle_cell_pos
     float dwv[3][3];
     if (PB) {
 #pragma unroll
@@ -935,62 +925,98 @@ __device__ __forceinline__ void g2p_gather(const SceneDev& S, const TileCtx<E>& 
 #pragma unroll
             for (int a = 0; a < 3; a++) dwv[k][a] = dwk(k, sc.f[a]);
     }
+    const float4* row = vel + (l0[2] * H + l0[1]) * H + l0[0];
 #pragma unroll
     for (int oz = 0; oz < 3; oz++)
 #pragma unroll
-        for (int oy = 0; oy < 3; oy++)
+        for (int oy = 0; oy < 3; oy++) {
+            float wxy[3];
+#pragma unroll
+            for (int ox = 0; ox < 3; ox++) wxy[ox] = fm(sc.w[ox][0], sc.w[oy][1]);
 #pragma unroll
             for (int ox = 0; ox < 3; ox++) {
-                int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
-                float4 c4 = vel[j];
+                float4 c4 = row[(oz * H + oy) * H + ox];
                 float cv[3] = {c4.x, c4.y, c4.z};
-                float wxy = fm(sc.w[ox][0], sc.w[oy][1]);
-                float wgt = fm(wxy, sc.w[oz][2]);
+                float wgt = fm(wxy[ox], sc.w[oz][2]);
 #pragma unroll
-                for (int k = 0; k < 3; k++) nv[k] = fa(nv[k], fm(wgt, cv[k]));
+                for (int k = 0; k < 3; k++) nv[k] = ff(wgt, cv[k], nv[k]);
                 if (!PB) {
                     float g[3];
                     g[0] = fm(fm(dwv[ox][0], sc.w[oy][1]), sc.w[oz][2]);
                     g[1] = fm(fm(sc.w[ox][0], dwv[oy][1]), sc.w[oz][2]);
-                    g[2] = fm(wxy, dwv[oz][2]);
+                    g[2] = fm(wxy[ox], dwv[oz][2]);
 #pragma unroll
                     for (int col = 0; col < 3; col++)
 #pragma unroll
-                        for (int r = 0; r < 3; r++) G[col * 3 + r] = fa(G[col * 3 + r], fm(g[col], cv[r]));
+                        for (int r = 0; r < 3; r++) G[col * 3 + r] = ff(g[col], cv[r], G[col * 3 + r]);
                 } else {
                     float wv[3] = {fm(wgt, cv[0]), fm(wgt, cv[1]), fm(wgt, cv[2])};
                     float dist[3] = {offs[0][ox], offs[1][oy], offs[2][oz]};
 #pragma unroll
                     for (int col = 0; col < 3; col++)
 #pragma unroll
-                        for (int r = 0; r < 3; r++) G[col * 3 + r] = fa(G[col * 3 + r], fm(wv[r], dist[col]));
+                        for (int r = 0; r < 3; r++) G[col * 3 + r] = ff(wv[r], dist[col], G[col * 3 + r]);
                 }
             }
+        }
 }
 
 template <bool PB>
-__device__ __forceinline__ void g2p_finish(const SceneDev& S, const float* nv, const float* G, PState& p) {
+__device__ __forceinline__ void g2p_finish(const SceneDev& S, const float* nv, const float* G, float* vel, float* dxp,
+                                           float* D) {
 #pragma unroll
-    for (int k = 0; k < 3; k++) { p.vel[k] = nv[k]; p.dxp[k] = fm(nv[k], S.dt); }
+    for (int k = 0; k < 3; k++) { vel[k] = nv[k]; dxp[k] = fm(nv[k], S.dt); }
     if (!PB) {
 #pragma unroll
-        for (int i = 0; i < 9; i++) p.D[i] = fm(G[i], S.dt);
+        for (int i = 0; i < 9; i++) D[i] = fm(G[i], S.dt);
     } else {
 #pragma unroll
-        for (int i = 0; i < 9; i++) p.D[i] = fm(fm(G[i], S.dt), 4.0f);
+        for (int i = 0; i < 9; i++) D[i] = fm(fm(G[i], S.dt), 4.0f);
     }
+}
+
+// Interaction force at grid cell cc (pbmpm.wgsl:104-134), added to f.
+__device__ __noinline__ void interaction_force(const SceneDev& S, const int* cc, float* f) {
+    float dv[3] = {fs(i2f(cc[0]), S.ipos[0]), fs(i2f(cc[1]), S.ipos[1]), fs(i2f(cc[2]), S.ipos[2])};
+    float dist = len3(dv);
+    if (!(dist < S.irad)) return;
+    float pd[3] = {0.f, 0.f, 1.f};
+    float l = len3(dv);
+    if (l > 0.001f) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) pd[k] = fd(dv[k], l);
+    }
+    float fl = fd(dist, S.irad);
+    float falloff = fs(1.0f, fm(fl, fl));
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float af = (S.imode == 0u) ? fm(fm(pd[k], S.istr), falloff)
+                                   : fm(fm(fm(-pd[k], S.istr), falloff), fs(1.0f, falloff));
+        f[k] = fa(f[k], af);
+    }
+}
+
+// i32((x * RN(1/dt)) * scale) and i32((x * dt) * scale), folded into one
+// product when the scale is a power of two (SceneDev::fold)
+template <bool FOLD>
+__device__ __forceinline__ int32_t enc_rdt(const SceneDev& S, float x) {
+    return FOLD ? f2i(fm(x, S.rdts)) : f2i(fm(fm(x, S.rdt), S.scale));
+}
+template <bool FOLD>
+__device__ __forceinline__ int32_t enc_dt(const SceneDev& S, float x) {
+    return FOLD ? f2i(fm(x, S.dts)) : f2i(fm(fm(x, S.dt), S.scale));
 }
 
 // affine P2G + particle-side forces (pbmpm.wgsl:41-147) into the shared tile.
 // WITH_MASS = false skips the mass adds: within one substep positions and
 // masses do not change between PBMPM iterations, so every iteration's mass
-// sums equal the first iteration's (the caller carries them over).
-template <int E, bool WITH_MASS = true>
-__device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const TileCtx<E>& T, const float* pos, float mass,
-                                                   const float* dxp, const float* D, uint32_t* acc) {
+// sums equal the first iteration's (the caller carries them over).  The
+// i32 adds commute, so the cells are visited in any order: (x, y) pairs
+// outside, z inside, sharing the partial affine sums of each pair.
+template <int E, bool WITH_MASS, bool FOLD>
+__device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const TileCtx<E>& T, const Stencil& sc,
+                                                   float mass, const float* dxp, const float* D, uint32_t* acc) {
     constexpr int H = E + 2, NC = H * H * H;
-    Stencil sc;
-    make_stencil(S, pos, sc);
     int l0[3];
     bool inside = true;
 #pragma unroll
@@ -999,72 +1025,58 @@ __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const Tile
         inside = inside && l0[k] >= 0 && l0[k] < E;
     }
     if (!inside) return;
-    // D * off with off = cell - particle_cell_pos; the three column products
-    // of each axis offset are formed once (same operands, same order as the
-    // per-cell matrix-vector product).
-    float pD[3][3][3];  // pD[axis][o][r] = D[axis][r] * off_axis[o]
+    float off[3][3];  // off[axis][o] = (cell + o - 1) - particle_cell_pos
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         float pcp = fs(fa(i2f(sc.cell[a]), sc.f[a]), 0.5f);
 #pragma unroll
-        for (int o = 0; o < 3; o++) {
-            float off = fs(i2f(sc.cell[a] + o - 1), pcp);
-#pragma unroll
-            for (int r = 0; r < 3; r++) pD[a][o][r] = fm(D[a * 3 + r], off);
-        }
+        for (int o = 0; o < 3; o++) off[a][o] = fs(i2f(sc.cell[a] + o - 1), pcp);
     }
     const bool iact = S.iact != 0u;
-    // the z loop stays rolled (code size); its per-z operands are picked by
-    // selects so no array is indexed at run time (which would spill it)
-#pragma unroll 1
-    for (int oz = 0; oz < 3; oz++) {
-        const float wz = oz == 0 ? sc.w[0][2] : (oz == 1 ? sc.w[1][2] : sc.w[2][2]);
-        float pz[3];
+    // a force component that is zero for every cell adds i32(0) = 0
+    bool fon[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) pz[k] = oz == 0 ? pD[2][0][k] : (oz == 1 ? pD[2][1][k] : pD[2][2][k]);
+    for (int k = 0; k < 3; k++) fon[k] = iact || S.gdiv[k] != 0.0f;
+    uint32_t* base = acc + (l0[2] * H + l0[1]) * H + l0[0];
 #pragma unroll
-        for (int oy = 0; oy < 3; oy++)
+    for (int oy = 0; oy < 3; oy++)
+#pragma unroll(FOLD ? 3 : 1)
+        for (int ox = 0; ox < 3; ox++) {
+            // aff[r] = fma(D[2][r], off_z, fma(D[1][r], off_y, D[0][r] * off_x))
+            float pxy[3];
 #pragma unroll
-            for (int ox = 0; ox < 3; ox++) {
-                float wgt = fm(fm(sc.w[ox][0], sc.w[oy][1]), wz);
+            for (int r = 0; r < 3; r++) pxy[r] = ff(D[3 + r], off[1][oy], fm(D[r], off[0][ox]));
+            float wxy = fm(sc.w[ox][0], sc.w[oy][1]);
+#pragma unroll
+            for (int oz = 0; oz < 3; oz++) {
+                float wgt = fm(wxy, sc.w[oz][2]);
                 float wm = fm(wgt, mass);
                 float fo[3] = {S.gdiv[0], S.gdiv[1], S.gdiv[2]};
                 if (iact) {
                     int cc[3] = {sc.cell[0] + ox - 1, sc.cell[1] + oy - 1, sc.cell[2] + oz - 1};
                     float f3[3] = {S.g[0], S.g[1], S.g[2]};
-                    float dv[3] = {fs(i2f(cc[0]), S.ipos[0]), fs(i2f(cc[1]), S.ipos[1]), fs(i2f(cc[2]), S.ipos[2])};
-                    float dist = len3(dv);
-                    if (dist < S.irad) {
-                        float pd[3] = {0.f, 0.f, 1.f};
-                        float l = len3(dv);
-                        if (l > 0.001f) {
+                    interaction_force(S, cc, f3);
 #pragma unroll
-                            for (int k = 0; k < 3; k++) pd[k] = fd(dv[k], l);
-                        }
-                        float fl = fd(dist, S.irad);
-                        float falloff = fs(1.0f, fm(fl, fl));
-#pragma unroll
-                        for (int k = 0; k < 3; k++) {
-                            float af = (S.imode == 0u) ? fm(fm(pd[k], S.istr), falloff)
-                                                       : fm(fm(fm(-pd[k], S.istr), falloff), fs(1.0f, falloff));
-                            f3[k] = fa(f3[k], af);
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < 3; k++) fo[k] = divm(f3[k], S.fdiv, S.rfdiv, S.mfdiv);
+                    for (int k = 0; k < 3; k++) fo[k] = fm(f3[k], S.rfdiv);
                 }
-                int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
+                uint32_t* cell = base + (oz * H + oy) * H + ox;
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    float aff = fa(fa(pD[0][ox][k], pD[1][oy][k]), pz[k]);
-                    float mom = div_dt(S, fm(wm, fa(dxp[k], aff)));
-                    float mc = fm(fm(fo[k], wm), S.dt);
-                    uint32_t v = (uint32_t)f2i(fm(mom, S.scale)) + (uint32_t)f2i(fm(mc, S.scale));
-                    atomicAdd(&acc[(k + 1) * NC + j], v);
+                    float aff = ff(D[6 + k], off[2][oz], pxy[k]);
+                    uint32_t v = (uint32_t)enc_rdt<FOLD>(S, fm(wm, fa(dxp[k], aff)));
+                    if (fon[k]) v += (uint32_t)enc_dt<FOLD>(S, fm(fo[k], wm));
+                    atomicAdd(cell + (k + 1) * NC, v);
                 }
-                if (WITH_MASS) atomicAdd(&acc[j], (uint32_t)f2i(fm(wm, S.scale)));
+                if (WITH_MASS) atomicAdd(cell, (uint32_t)f2i(fm(wm, S.scale)));
             }
-    }
+        }
+}
+
+template <int E, bool WITH_MASS>
+__device__ __forceinline__ void p2g_pbmpm(const SceneDev& S, const TileCtx<E>& T, const Stencil& sc, float mass,
+                                          const float* dxp, const float* D, uint32_t* acc) {
+    if (S.fold) p2g_pbmpm_particle<E, WITH_MASS, true>(S, T, sc, mass, dxp, D, acc);
+    else p2g_pbmpm_particle<E, WITH_MASS, false>(S, T, sc, mass, dxp, D, acc);
 }
 
 template <int E>
@@ -1131,6 +1143,7 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
             for (int k = 0; k < 3; k++)
 #pragma unroll
                 for (int a = 0; a < 3; a++) dw[k][a] = dwk(k, sc.f[a]);
+            uint32_t* base = acc + (l0[2] * H + l0[1]) * H + l0[0];
 #pragma unroll 1
             for (int oz = 0; oz < 3; oz++) {
                 const float wz = oz == 0 ? sc.w[0][2] : (oz == 1 ? sc.w[1][2] : sc.w[2][2]);
@@ -1142,18 +1155,18 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
                         float wxy = fm(sc.w[ox][0], sc.w[oy][1]);
                         float wgt = fm(wxy, wz);
                         float g[3];
-                        g[0] = div_cd(S, fm(fm(dw[ox][0], sc.w[oy][1]), wz), 0);
-                        g[1] = div_cd(S, fm(fm(sc.w[ox][0], dw[oy][1]), wz), 1);
-                        g[2] = div_cd(S, fm(wxy, dwz), 2);
+                        g[0] = fm(fm(fm(dw[ox][0], sc.w[oy][1]), wz), S.rcd[0]);
+                        g[1] = fm(fm(fm(sc.w[ox][0], dw[oy][1]), wz), S.rcd[1]);
+                        g[2] = fm(fm(wxy, dwz), S.rcd[2]);
                         float sf[3];
                         mv3(M, g, sf);
-                        int j = ((l0[2] + oz) * H + (l0[1] + oy)) * H + (l0[0] + ox);
+                        uint32_t* cell = base + (oz * H + oy) * H + ox;
 #pragma unroll
                         for (int k = 0; k < 3; k++) {
-                            float mom = fa(fm(wgt, pm[k]), fm(sf[k], S.dt));
-                            atomicAdd(&acc[(k + 1) * NC + j], (uint32_t)f2i(fm(mom, S.scale)));
+                            float mom = ff(wgt, pm[k], fm(sf[k], S.dt));
+                            atomicAdd(cell + (k + 1) * NC, (uint32_t)f2i(fm(mom, S.scale)));
                         }
-                        atomicAdd(&acc[j], (uint32_t)f2i(fm(fm(wgt, p.mass), S.scale)));
+                        atomicAdd(cell, (uint32_t)f2i(fm(fm(wgt, p.mass), S.scale)));
                     }
             }
         }
@@ -1169,8 +1182,6 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
 // ------------------------------------------------------------------
 template <int E, bool PB, int BS>
 __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
-    constexpr int H = E + 2, NC = H * H * H;
-    (void)NC;
     extern __shared__ uint4 smem_raw[];
     int4* cell = reinterpret_cast<int4*>(smem_raw);
     const float4* vel = reinterpret_cast<const float4*>(smem_raw);
@@ -1195,8 +1206,8 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
             Stencil sc;
             make_stencil(S, p.pos, sc);
             float nv[3], G[9];
-            g2p_gather<E, PB>(S, T, vel, sc, nv, G);
-            g2p_finish<PB>(S, nv, G, p);
+            g2p_gather<E, PB>(T, vel, sc, nv, G);
+            g2p_finish<PB>(S, nv, G, p.vel, p.dxp, p.D);
             integrate(S, p, c.counters);
             store_particle(rec, p);
         }
@@ -1206,8 +1217,34 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
 
 // ------------------------------------------------------------------
 // PBMPM first iteration: constraints + affine P2G + forces
-// (pbmpm.wgsl:154-178)
+// (pbmpm.wgsl:154-178); writes the iteration records
 // ------------------------------------------------------------------
+__device__ __forceinline__ void store_iter_rec(const Ctx& c, uint32_t t, const float* pos, float mass, const float* Fe,
+                                               const float* Fei, float relax) {
+    float4* r = c.iter_rec + t;
+    const size_t n = c.n_particles;
+    r[0] = make_float4(pos[0], pos[1], pos[2], mass);
+    r[n] = make_float4(Fe[0], Fe[1], Fe[2], Fe[3]);
+    r[2 * n] = make_float4(Fe[4], Fe[5], Fe[6], Fe[7]);
+    r[3 * n] = make_float4(Fe[8], Fei[0], Fei[1], Fei[2]);
+    r[4 * n] = make_float4(Fei[3], Fei[4], Fei[5], Fei[6]);
+    r[5 * n] = make_float4(Fei[7], Fei[8], relax, 0.f);
+}
+
+__device__ __forceinline__ void load_iter_rec(const Ctx& c, uint32_t t, float* pos, float& mass, float* Fe,
+                                              float* Fei, float& relax) {
+    const float4* r = c.iter_rec + t;
+    const size_t n = c.n_particles;
+    float4 q0 = __ldg(r), q1 = __ldg(r + n), q2 = __ldg(r + 2 * n), q3 = __ldg(r + 3 * n), q4 = __ldg(r + 4 * n),
+           q5 = __ldg(r + 5 * n);
+    pos[0] = q0.x; pos[1] = q0.y; pos[2] = q0.z; mass = q0.w;
+    Fe[0] = q1.x; Fe[1] = q1.y; Fe[2] = q1.z; Fe[3] = q1.w;
+    Fe[4] = q2.x; Fe[5] = q2.y; Fe[6] = q2.z; Fe[7] = q2.w;
+    Fe[8] = q3.x; Fei[0] = q3.y; Fei[1] = q3.z; Fei[2] = q3.w;
+    Fei[3] = q4.x; Fei[4] = q4.y; Fei[5] = q4.z; Fei[6] = q4.w;
+    Fei[7] = q5.x; Fei[8] = q5.y; relax = q5.z;
+}
+
 template <int E, int BS>
 __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
@@ -1226,8 +1263,14 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
             uint32_t pid = c.sorted[begin + i];
             PState p;
             load_particle<true>(c.particles + (size_t)pid * 12, p, false, true);
-            pbmpm_constraints(S, p.Fe, p.Fp, p.D);
-            p2g_pbmpm_particle<E>(S, T, p.pos, p.mass, p.dxp, p.D, acc);
+            float Fei[9];
+            inv3(p.Fe, Fei);
+            float relax = pbmpm_relax(S, p.Fp);
+            store_iter_rec(c, begin + i, p.pos, p.mass, p.Fe, Fei, relax);
+            pbmpm_constraints(S, p.Fe, Fei, relax, p.D);
+            Stencil sc;
+            make_stencil(S, p.pos, sc);
+            p2g_pbmpm<E, true>(S, T, sc, p.mass, p.dxp, p.D, acc);
         }
         __syncthreads();
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
@@ -1235,7 +1278,8 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
     }
 }
 
-// PBMPM iteration i>0: G2P of iteration i-1, constraints, P2G of iteration i
+// PBMPM iteration i>0: G2P of iteration i-1, constraints, P2G of iteration i,
+// all from the iteration records (contiguous in tile order)
 template <int E, int BS>
 __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
@@ -1258,16 +1302,15 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
-            uint32_t pid = c.sorted[begin + i];
-            PState p;
-            load_particle<true>(c.particles + (size_t)pid * 12, p, false, false);
+            float pos[3], mass, Fe[9], Fei[9], relax;
+            load_iter_rec(c, begin + i, pos, mass, Fe, Fei, relax);
             Stencil sc;
-            make_stencil(S, p.pos, sc);
-            float nv[3], G[9];
-            g2p_gather<E, true>(S, T, vel, sc, nv, G);
-            g2p_finish<true>(S, nv, G, p);
-            pbmpm_constraints(S, p.Fe, p.Fp, p.D);
-            p2g_pbmpm_particle<E, false>(S, T, p.pos, p.mass, p.dxp, p.D, acc);
+            make_stencil(S, pos, sc);
+            float nv[3], G[9], v[3], dxp[3], D[9];
+            g2p_gather<E, true>(T, vel, sc, nv, G);
+            g2p_finish<true>(S, nv, G, v, dxp, D);
+            pbmpm_constraints(S, Fe, Fei, relax, D);
+            p2g_pbmpm<E, false>(S, T, sc, mass, dxp, D, acc);
         }
         __syncthreads();
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
@@ -1300,11 +1343,11 @@ __global__ void __launch_bounds__(256) k_grid_dense(Ctx c, uint32_t scene, int a
             if (apply_update) {
                 float cm = inv_s(S, s.x);
                 if (cm > 0.0f) {
-                    CellDiv dm(cm);
+                    float rm = __frcp_rn(cm);
                     int32_t mi[3] = {s.y, s.z, s.w};
                     float u[3];
 #pragma unroll
-                    for (int k = 0; k < 3; k++) u[k] = fa(dm(inv_s(S, mi[k])), S.gdt[k]);
+                    for (int k = 0; k < 3; k++) u[k] = fa(fm(inv_s(S, mi[k]), rm), S.gdt[k]);
                     grid_bc(S, gc, u);
                     s.y = f2i(fm(fm(u[0], cm), S.scale));
                     s.z = f2i(fm(fm(u[1], cm), S.scale));
@@ -1326,22 +1369,26 @@ __device__ __forceinline__ uint32_t mix32(uint64_t v) {
     return (uint32_t)v;
 }
 
-// Compares divc against __fdiv_rn on n pseudo-random operand pairs (random
-// sign, exponent in [-60, 60], mantissa) and checks the f32 -> i32
-// conversion on NaN, infinities and out-of-range values.  counts[0] = division
-// mismatches, counts[1] = conversion mismatches, counts[2] = the raw hardware
-// conversion of a NaN (informational).
+// Checks, on n pseudo-random operand pairs, the two identities the kernels
+// rely on: the folded fixed-point encoding i32(x * (r * 2^k)) equals
+// i32((x * r) * 2^k) for 0 <= k <= 60 (x with exponent in [-80, 40], r in
+// [2^-30, 2^30]), and the reciprocal __frcp_rn(d) equals the IEEE quotient
+// 1 / d; also the f32 -> i32 conversion on NaN, infinities and out-of-range
+// values.  counts[0] = identity mismatches, counts[1] = conversion mismatch
+// code, counts[2] = the raw hardware conversion of a NaN (informational).
 __global__ void k_selftest(uint64_t n, uint64_t seed, unsigned long long* counts) {
     uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     unsigned long long bad = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         uint32_t a = mix32(seed ^ (i * 2 + 0)), b = mix32(seed ^ (i * 2 + 1));
-        int ex = (int)(a % 121u) - 60, ed = (int)((a >> 8) % 81u) - 40;
+        int ex = (int)(a % 121u) - 80, er = (int)((a >> 8) % 61u) - 30, k = (int)((a >> 16) % 61u);
         float x = __uint_as_float((a & 0x80000000u) | ((uint32_t)(ex + 127) << 23) | (b & 0x7fffffu));
-        float d = __uint_as_float(((uint32_t)(ed + 127) << 23) | ((b >> 9) & 0x7fffffu) | ((a & 1u) << 22));
-        if (i & 1) d = -d;
-        float r = __frcp_rn(d);
-        if (__float_as_uint(divc(x, d, r)) != __float_as_uint(__fdiv_rn(x, d))) bad++;
+        float r = __uint_as_float(((uint32_t)(er + 127) << 23) | ((b >> 9) & 0x7fffffu) | ((a & 1u) << 22));
+        if (i & 1) r = -r;
+        float p2 = __uint_as_float((uint32_t)(k + 127) << 23);
+        float rk = __fmul_rn(r, p2);
+        if (f2i(__fmul_rn(__fmul_rn(x, r), p2)) != f2i(__fmul_rn(x, rk))) bad++;
+        if (__float_as_uint(__frcp_rn(r)) != __float_as_uint(__fdiv_rn(1.0f, r))) bad++;
     }
     if (bad) atomicAdd(&counts[0], bad);
     if (blockIdx.x == 0 && threadIdx.x == 0) {

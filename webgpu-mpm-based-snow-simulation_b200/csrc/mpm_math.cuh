@@ -2,15 +2,24 @@
 //
 // Every helper fixes one evaluation order so the f32 results, and therefore
 // the i32 fixed-point grid, are reproducible bit for bit.  The kernels are
-// compiled with -fmad=false (no contraction of a*b+c), IEEE division and
-// square root, and without flush-to-zero.
+// compiled with -fmad=false (the compiler fuses nothing on its own), IEEE
+// division and square root, and without flush-to-zero; every fused
+// multiply-add below is an explicit __fmaf_rn.
 //
-// Conventions (WGSL semantics of the reference shaders):
+// Canonical rules (WGSL leaves fusion and the rounding of division, exp and
+// pow to the implementation; division is specified to 2.5 ulp):
 //   mat3 is column-major, m[c*3 + r] = M[c][r]; constructors take columns
-//   dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z
-//   (M*v)[r] = (M[0][r]*v.x + M[1][r]*v.y) + M[2][r]*v.z
-//   (A*B)[c][r] = (A[0][r]*B[c][0] + A[1][r]*B[c][1]) + A[2][r]*B[c][2]
-//   det(M) = (M00*(M11*M22 - M21*M12) - M10*(M01*M22 - M21*M02)) + M20*(M01*M12 - M11*M02)
+//   dot(a,b)     = fma(a.z, b.z, fma(a.y, b.y, a.x*b.x))
+//   (M*v)[r]     = fma(M[2][r], v.z, fma(M[1][r], v.y, M[0][r]*v.x))
+//   (A*B)[c][r]  = fma(A[2][r], B[c][2], fma(A[1][r], B[c][1], A[0][r]*B[c][0]))
+//   cross(a,b).x = fma(a.y, b.z, -(a.z*b.y)), and cyclically
+//   det(M)       = fma(M20, k2, fma(-M10, k1, M00*k0)),
+//                  k0 = fma(M11,M22,-(M21*M12)), k1 = fma(M01,M22,-(M21*M02)), k2 = fma(M01,M12,-(M11*M02))
+//   s += a*b in the transfer sums = fma(a, b, s)
+//   x / d, d constant over a substep (dt, cell size, fixed-point scale,
+//     force divisor) = x * RN(1/d), the reciprocal rounded once on the host
+//   momentum / cell mass = momentum * RN(1/mass)
+//   other divisions and sqrt are IEEE
 //   i32(f): truncation toward zero, saturating, NaN -> 0
 //   exp/pow: f64 evaluation by exp64/log64 below, rounded once to f32
 #pragma once
@@ -117,54 +126,24 @@ __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); 
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
 
-// Correctly rounded x / d from the correctly rounded reciprocal r = RN(1/d),
-// for a divisor d in [2^-40, 2^40].  q0 = RN(x r) is within two ulps of x/d;
-// one correction q1 = RN(q0 + (x - d q0) r) makes it faithful; a second
-// correction with the (exact, fused) residual of q1 then returns RN(x/d) by
-// the correction theorem of P. Markstein (IBM J. Res. Dev. 34(1), 1990):
-// a faithful quotient plus a reciprocal within half an ulp give the
-// correctly rounded quotient.  Quotients outside [2^-40, 2^40], zeros,
-// infinities and NaNs take the IEEE division, so no residual can underflow.
-// The result equals __fdiv_rn(x, d) bit for bit; a device self-test checks
-// it on random operands.
-__device__ __forceinline__ float divc(float x, float d, float r) {
-    float q = __fmul_rn(x, r);
-    float a = fabsf(q);
-    if (!(a >= 0x1p-40f && a <= 0x1p40f)) return __fdiv_rn(x, d);
-    float e = __fmaf_rn(-q, d, x);
-    q = __fmaf_rn(e, r, q);
-    e = __fmaf_rn(-q, d, x);
-    return __fmaf_rn(e, r, q);
-}
-// Division modes for a divisor that is constant over a launch:
-//   DIV_IEEE  plain IEEE division
-//   DIV_CORR  corrected reciprocal (divc), |d| in [2^-40, 2^40]
-//   DIV_POW2  d = 2^k with k <= 0: x * 2^-k is exact for every x (scaling by
-//             a power of two >= 1 loses no bits), so it equals x / d
-//   DIV_POW2S d = 2^k with 0 < k <= 100, used only for integer-valued x
-//             (|x| >= 1 or 0): x * 2^-k stays normal, hence exact
-enum DivMode : uint32_t { DIV_IEEE = 0, DIV_CORR = 1, DIV_POW2 = 2, DIV_POW2S = 3 };
-__device__ __forceinline__ float divm(float x, float d, float r, uint32_t mode) {
-    if (mode >= DIV_POW2) return __fmul_rn(x, r);
-    return mode == DIV_CORR ? divc(x, d, r) : __fdiv_rn(x, d);
-}
+__device__ __forceinline__ float ff(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
 __device__ __forceinline__ float dot3(const float* a, const float* b) {
-    return fa(fa(fm(a[0], b[0]), fm(a[1], b[1])), fm(a[2], b[2]));
+    return ff(a[2], b[2], ff(a[1], b[1], fm(a[0], b[0])));
 }
 __device__ __forceinline__ void cross3(const float* a, const float* b, float* o) {
-    float x = fs(fm(a[1], b[2]), fm(a[2], b[1]));
-    float y = fs(fm(a[2], b[0]), fm(a[0], b[2]));
-    float z = fs(fm(a[0], b[1]), fm(a[1], b[0]));
+    float x = ff(a[1], b[2], -fm(a[2], b[1]));
+    float y = ff(a[2], b[0], -fm(a[0], b[2]));
+    float z = ff(a[0], b[1], -fm(a[1], b[0]));
     o[0] = x; o[1] = y; o[2] = z;
 }
 __device__ __forceinline__ float len3(const float* a) { return __fsqrt_rn(dot3(a, a)); }
 
 __device__ __forceinline__ float det3(const float* m) {
-    float t0 = fm(m[0], fs(fm(m[4], m[8]), fm(m[7], m[5])));
-    float t1 = fm(m[3], fs(fm(m[1], m[8]), fm(m[7], m[2])));
-    float t2 = fm(m[6], fs(fm(m[1], m[5]), fm(m[4], m[2])));
-    return fa(fs(t0, t1), t2);
+    float k0 = ff(m[4], m[8], -fm(m[7], m[5]));
+    float k1 = ff(m[1], m[8], -fm(m[7], m[2]));
+    float k2 = ff(m[1], m[5], -fm(m[4], m[2]));
+    return ff(m[6], k2, ff(-m[3], k1, fm(m[0], k0)));
 }
 
 // mat3x3Inverse (matrixOps.wgsl:8-27): adjugate * (1/det); identity if det == 0.
@@ -174,15 +153,15 @@ __device__ __forceinline__ void inv3(const float* m, float* o) {
         o[0] = 1.f; o[1] = 0.f; o[2] = 0.f; o[3] = 0.f; o[4] = 1.f; o[5] = 0.f; o[6] = 0.f; o[7] = 0.f; o[8] = 1.f;
         return;
     }
-    float a0 = fs(fm(m[4], m[8]), fm(m[5], m[7]));
-    float a1 = fs(fm(m[2], m[7]), fm(m[1], m[8]));
-    float a2 = fs(fm(m[1], m[5]), fm(m[2], m[4]));
-    float a3 = fs(fm(m[5], m[6]), fm(m[3], m[8]));
-    float a4 = fs(fm(m[0], m[8]), fm(m[2], m[6]));
-    float a5 = fs(fm(m[2], m[3]), fm(m[0], m[5]));
-    float a6 = fs(fm(m[3], m[7]), fm(m[4], m[6]));
-    float a7 = fs(fm(m[1], m[6]), fm(m[0], m[7]));
-    float a8 = fs(fm(m[0], m[4]), fm(m[1], m[3]));
+    float a0 = ff(m[4], m[8], -fm(m[5], m[7]));
+    float a1 = ff(m[2], m[7], -fm(m[1], m[8]));
+    float a2 = ff(m[1], m[5], -fm(m[2], m[4]));
+    float a3 = ff(m[5], m[6], -fm(m[3], m[8]));
+    float a4 = ff(m[0], m[8], -fm(m[2], m[6]));
+    float a5 = ff(m[2], m[3], -fm(m[0], m[5]));
+    float a6 = ff(m[3], m[7], -fm(m[4], m[6]));
+    float a7 = ff(m[1], m[6], -fm(m[0], m[7]));
+    float a8 = ff(m[0], m[4], -fm(m[1], m[3]));
     float s = fd(1.0f, det);
     o[0] = fm(a0, s); o[1] = fm(a1, s); o[2] = fm(a2, s);
     o[3] = fm(a3, s); o[4] = fm(a4, s); o[5] = fm(a5, s);
@@ -201,15 +180,15 @@ __device__ __forceinline__ void mul3(const float* A, const float* B, float* o) {
     for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int r = 0; r < 3; r++)
-            t[c * 3 + r] = fa(fa(fm(A[r], B[c * 3 + 0]), fm(A[3 + r], B[c * 3 + 1])), fm(A[6 + r], B[c * 3 + 2]));
+            t[c * 3 + r] = ff(A[6 + r], B[c * 3 + 2], ff(A[3 + r], B[c * 3 + 1], fm(A[r], B[c * 3 + 0])));
 #pragma unroll
     for (int i = 0; i < 9; i++) o[i] = t[i];
 }
 
 __device__ __forceinline__ void mv3(const float* M, const float* v, float* o) {
-    float t0 = fa(fa(fm(M[0], v[0]), fm(M[3], v[1])), fm(M[6], v[2]));
-    float t1 = fa(fa(fm(M[1], v[0]), fm(M[4], v[1])), fm(M[7], v[2]));
-    float t2 = fa(fa(fm(M[2], v[0]), fm(M[5], v[1])), fm(M[8], v[2]));
+    float t0 = ff(M[6], v[2], ff(M[3], v[1], fm(M[0], v[0])));
+    float t1 = ff(M[7], v[2], ff(M[4], v[1], fm(M[1], v[0])));
+    float t2 = ff(M[8], v[2], ff(M[5], v[1], fm(M[2], v[0])));
     o[0] = t0; o[1] = t1; o[2] = t2;
 }
 
@@ -237,7 +216,7 @@ __device__ __forceinline__ void xform_point(const float* M, const float* v, floa
     float t[3];
 #pragma unroll
     for (int r = 0; r < 3; r++)
-        t[r] = fa(fa(fa(fm(M[r], v[0]), fm(M[4 + r], v[1])), fm(M[8 + r], v[2])), fm(M[12 + r], 1.0f));
+        t[r] = fa(ff(M[8 + r], v[2], ff(M[4 + r], v[1], fm(M[r], v[0]))), M[12 + r]);
     o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
 }
 
