@@ -31,7 +31,8 @@ using namespace mpm;
 
 static const char* kKernelNames[K_COUNT] = {
     "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
-    "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense"};
+    "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense",
+    "tile_nbr"};
 
 struct TimedLaunch {
     uint32_t kid;
@@ -80,6 +81,7 @@ struct MpmHandle {
     uint32_t* chunk_nst = nullptr;
     uint32_t* chunk_np = nullptr;
     int4* tiles[2] = {nullptr, nullptr};
+    int32_t* st_nbr = nullptr;    // max_tiles x 27 neighbour indices
     float4* iter_rec = nullptr;   // PBMPM iteration records, IR_PLANES x N float4
     int last_tiles = 0;
     SceneDev* d_scenes = nullptr;
@@ -286,7 +288,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     for (auto e : h->event_pool) cudaEventDestroy(e);
     void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
-                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters, h->iter_rec};
+                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters, h->iter_rec, h->st_nbr};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h->own_particles && h->particles) cudaFree(h->particles);
@@ -331,10 +333,12 @@ static int alloc_table(MpmHandle* h, uint32_t cap) {
 static int alloc_tiles(MpmHandle* h, uint32_t n) {
     for (int i = 0; i < 2; i++)
         if (h->tiles[i]) { cudaFree(h->tiles[i]); h->tiles[i] = nullptr; }
+    if (h->st_nbr) { cudaFree(h->st_nbr); h->st_nbr = nullptr; }
     size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     h->max_tiles = n;
     CK(h, cudaMalloc(&h->tiles[0], (size_t)n * NC * 16));
     CK(h, cudaMalloc(&h->tiles[1], (size_t)n * NC * 16));
+    CK(h, cudaMalloc(&h->st_nbr, (size_t)n * 27 * 4));
     destroy_graphs(h);
     return MPM_OK;
 }
@@ -599,6 +603,7 @@ static Ctx make_ctx(MpmHandle* h, int parity) {
     c.tiles_a = h->tiles[0];
     c.tiles_b = h->tiles[0];
     c.iter_rec = h->iter_rec;
+    c.st_nbr = h->st_nbr;
     c.scenes = h->d_scenes;
     c.scene_first = h->d_scene_first;
     c.counters = h->counters;
@@ -669,6 +674,7 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
     L(K_COMPACT_B);
     L(K_COMPACT_C);
     L(K_BIN_SCATTER);
+    L(K_TILE_NBR);
     if (method == MPM_METHOD_EXPLICIT) {
         c.tiles_a = h->tiles[0];
         L(K_P2G_EXPLICIT);
@@ -976,7 +982,8 @@ constexpr size_t NA_CHUNK_NP = NA_CHUNK_NST + na_round(NA_H / COMPACT_CHUNK * 4)
 constexpr size_t NA_TILES0 = NA_CHUNK_NP + na_round(NA_H / COMPACT_CHUNK * 4);  // halo sums, int4
 constexpr size_t NA_TILES1 = NA_TILES0 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
 constexpr size_t NA_ITER_REC = NA_TILES1 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);  // PBMPM records
-constexpr size_t NA_SCENE = NA_ITER_REC + na_round(NA_P * IR_PLANES * 16);
+constexpr size_t NA_ST_NBR = NA_ITER_REC + na_round(NA_P * IR_PLANES * 16);  // tile neighbour table
+constexpr size_t NA_SCENE = NA_ST_NBR + na_round(MPM_NOALLOC_MAX_TILES * 27 * 4);
 constexpr size_t NA_SCENE_FIRST = NA_SCENE + na_round(sizeof(SceneDev));
 constexpr size_t NA_COUNTERS = NA_SCENE_FIRST + na_round(2 * 4);
 constexpr size_t NA_BYTES = NA_COUNTERS + na_round(sizeof(Counters));
@@ -1104,6 +1111,7 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     c.tiles_a = tiles[0];
     c.tiles_b = tiles[0];
     c.iter_rec = (float4*)(b + NA_ITER_REC);
+    c.st_nbr = (int32_t*)(b + NA_ST_NBR);
     c.scenes = (const SceneDev*)(b + NA_SCENE);
     c.scene_first = (const uint32_t*)(b + NA_SCENE_FIRST);
     c.counters = (Counters*)(b + NA_COUNTERS);
@@ -1131,7 +1139,7 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
         int grid = std::max(1, D.n_sms * std::max(1, D.blocks_per_sm[kid]));
         return launch_kernel<NA_EDGE>(kid, c, s, grid, 0, 0, nullptr);
     };
-    for (uint32_t k : {K_BIN_INSERT, K_COMPACT_A, K_COMPACT_B, K_COMPACT_C, K_BIN_SCATTER}) NA_CK(run(k));
+    for (uint32_t k : {K_BIN_INSERT, K_COMPACT_A, K_COMPACT_B, K_COMPACT_C, K_BIN_SCATTER, K_TILE_NBR}) NA_CK(run(k));
     if (method == MPM_METHOD_EXPLICIT) {
         NA_CK(run(K_P2G_EXPLICIT));
         NA_CK(run(K_G2P_EXPLICIT));

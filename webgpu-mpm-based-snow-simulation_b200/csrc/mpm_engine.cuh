@@ -14,6 +14,9 @@
 //   tiles[2]    max_tiles x (E+2)^3 x int4   per-tile halo sums
 //               (mass, momentum x, y, z) in the reference i32 fixed point
 //   iter_rec    IR_PLANES x N float4         PBMPM iteration records (below)
+//   st_nbr      max_tiles x 27 i32           compact index of each tile's 27
+//                                            neighbours (d = 9(dz+1) + 3(dy+1) + dx+1),
+//                                            built once per substep after binning
 //
 // A tile is E^3 grid cells (E = 8, 12 or 16, i.e. 2^3, 3^3 or 4^3 of the reference's
 // 4^3-cell blocks).  Its P2G writes the (E+2)^3 halo region it touches; the
@@ -113,6 +116,7 @@ struct Ctx {
     int4* tiles_a;            // tiles written by this pass's P2G
     int4* tiles_b;            // tiles read by this pass's G2P
     float4* iter_rec;         // PBMPM iteration records, IR_PLANES x n float4, sorted order
+    int32_t* st_nbr;          // per compact tile, the compact index of its 27 neighbours (-1: none)
     const SceneDev* scenes;
     const uint32_t* scene_first;  // n_scenes + 1 particle offsets
     Counters* counters;
@@ -146,6 +150,7 @@ enum KernelId : uint32_t {
     K_PBMPM_ITER,
     K_G2P_PBMPM,
     K_GRID_DENSE,
+    K_TILE_NBR,
     K_COUNT
 };
 

@@ -727,23 +727,10 @@ __device__ __forceinline__ int4 assemble_cell(const int4* tiles, const int* nbr,
     return s;
 }
 
-template <int E>
-__device__ __forceinline__ void lookup_neighbors(const Ctx& c, const TileCtx<E>& T, uint32_t st, int* nbr) {
-    if (threadIdx.x < 27) {
-        int d = threadIdx.x;
-        int dx = d % 3 - 1, dy = (d / 3) % 3 - 1, dz = d / 9 - 1;
-        int r;
-        if (d == 13) {
-            r = (int)st;
-        } else {
-            int sx = T.origin[0] / E + dx, sy = T.origin[1] / E + dy, sz = T.origin[2] / E + dz;
-            uint64_t nk = pack_key(T.scene, sx, sy, sz);
-            uint32_t slot = tile_lookup(c, nk, T.scene, sx, sy, sz);
-            r = (slot == INVALID) ? -1 : (int)c.slot_st[slot];
-            if (r >= (int)c.max_tiles) r = -1;
-        }
-        nbr[d] = r;
-    }
+// Compact indices of this tile's 27 neighbours (built by k_tile_nbr) into
+// shared memory; d = 9(dz+1) + 3(dy+1) + (dx+1), -1 where no tile exists.
+__device__ __forceinline__ void load_neighbors(const Ctx& c, uint32_t st, int* nbr) {
+    if (threadIdx.x < 27) nbr[threadIdx.x] = __ldg(&c.st_nbr[(size_t)st * 27u + threadIdx.x]);
 }
 
 // Cell velocity the G2P kernels read.  Explicit mode first applies the grid
@@ -787,23 +774,23 @@ struct HaloEntries {
 };
 
 template <int E>
-__device__ __forceinline__ void halo_entry(int e, int& d, int& j, int& jj) {
+__host__ __device__ constexpr void halo_entry(int e, int& d, int& j, int& jj) {
     constexpr int H = E + 2;
     using HE = HaloEntries<E>;
-    int dx, dy, dz, ix, iy, iz;
+    int dx = 0, dy = 0, dz = 0, ix = 0, iy = 0, iz = 0;
     if (e < HE::NF) {
         int r = e / HE::FACE, o = e - r * HE::FACE;
         int axis = r >> 1, sg = (r & 1) ? 1 : -1;
-        if (axis == 0) { ix = o & 1; iy = (o >> 1) % H; iz = (o >> 1) / H; dx = sg; dy = 0; dz = 0; }
-        else if (axis == 1) { ix = o % H; iy = (o / H) & 1; iz = o / (2 * H); dx = 0; dy = sg; dz = 0; }
-        else { ix = o % H; iy = (o / H) % H; iz = o / (H * H); dx = 0; dy = 0; dz = sg; }
+        if (axis == 0) { ix = o & 1; iy = (o >> 1) % H; iz = (o >> 1) / H; dx = sg; }
+        else if (axis == 1) { ix = o % H; iy = (o / H) & 1; iz = o / (2 * H); dy = sg; }
+        else { ix = o % H; iy = (o / H) % H; iz = o / (H * H); dz = sg; }
     } else if (e < HE::NF + HE::NED) {
         int e2 = e - HE::NF;
         int r = e2 / HE::EDGE, o = e2 - r * HE::EDGE;
         int za = r >> 2, s1 = (r & 1) ? 1 : -1, s2 = (r & 2) ? 1 : -1;
-        if (za == 0) { ix = o % H; iy = (o / H) & 1; iz = o / (2 * H); dx = 0; dy = s1; dz = s2; }
-        else if (za == 1) { ix = o & 1; iy = (o >> 1) % H; iz = (o >> 1) / H; dx = s1; dy = 0; dz = s2; }
-        else { ix = o & 1; iy = (o >> 1) & 1; iz = o >> 2; dx = s1; dy = s2; dz = 0; }
+        if (za == 0) { ix = o % H; iy = (o / H) & 1; iz = o / (2 * H); dy = s1; dz = s2; }
+        else if (za == 1) { ix = o & 1; iy = (o >> 1) % H; iz = (o >> 1) / H; dx = s1; dz = s2; }
+        else { ix = o & 1; iy = (o >> 1) & 1; iz = o >> 2; dx = s1; dy = s2; }
     } else {
         int o = e - HE::NF - HE::NED;
         int r = o >> 3;
@@ -817,49 +804,77 @@ __device__ __forceinline__ void halo_entry(int e, int& d, int& j, int& jj) {
     d = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
 }
 
+// The halo entries decoded once, at compile time: entry e packs its
+// neighbour direction d (5 bits), its cell j in this tile's region (13 bits)
+// and the cell jj in the neighbour's region (13 bits).
+template <int E>
+struct HaloTable {
+    uint32_t v[HaloEntries<E>::N];
+};
+static_assert((18 * 18 * 18) < (1 << 13), "halo cell index must fit 13 bits");
+
+template <int E>
+__host__ __device__ constexpr HaloTable<E> make_halo_table() {
+    HaloTable<E> t{};
+    for (int e = 0; e < HaloEntries<E>::N; e++) {
+        int d = 0, j = 0, jj = 0;
+        halo_entry<E>(e, d, j, jj);
+        t.v[e] = (uint32_t)d | ((uint32_t)j << 5) | ((uint32_t)jj << 18);
+    }
+    return t;
+}
+
+__device__ const HaloTable<8> g_halo8 = make_halo_table<8>();
+__device__ const HaloTable<12> g_halo12 = make_halo_table<12>();
+__device__ const HaloTable<16> g_halo16 = make_halo_table<16>();
+
+template <int E>
+__device__ __forceinline__ const uint32_t* halo_table() {
+    return E == 8 ? g_halo8.v : (E == 12 ? g_halo12.v : g_halo16.v);
+}
+
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
     uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Sum this tile's halo region: the tile's own (E+2)^3 sums (asynchronous
-// 16-byte copies, all in flight at once) plus the overlapping parts of the
-// neighbour halos (loaded in batches of U per thread before their shared
-// i32 atomic adds, so the loads overlap).  Leaves the int4 sums in `cell`.
-template <int E, int U, bool COPY_MASS = false>
+// Sum this tile's halo region into `cell`: the tile's own (E+2)^3 sums
+// (asynchronous 16-byte copies, all in flight at once) plus the overlapping
+// parts of the neighbour halos (entries of the compile-time halo table,
+// loaded into registers in batches of U per thread and added with shared
+// i32 atomics).  The first batch of neighbour loads is issued before the
+// wait for the copies, so both latencies overlap.  COPY_MASS also keeps this
+// tile's own halo mass sums in own_mass (before the neighbour sums land).
+template <int E, int BS, bool COPY_MASS = false>
 __device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr, int4* cell,
                                               uint32_t* own_mass = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
     constexpr int NE = HaloEntries<E>::N;
+    constexpr int PER = (NE + BS - 1) / BS;      // entries per thread
+    constexpr int U = PER <= 10 ? PER : 8;       // entries per register batch
     const int4* own = tiles + (size_t)nbr[13] * NC;
-    for (int j = threadIdx.x; j < NC; j += blockDim.x) cp_async16(&cell[j], own + j);
-    cp_async_wait_all();
-    __syncthreads();
-    if (COPY_MASS) {
-        // this tile's own halo mass sums, kept before the neighbour sums are added
-        for (int j = threadIdx.x; j < NC; j += blockDim.x) own_mass[j] = (uint32_t)cell[j].x;
-        __syncthreads();
-    }
-    const int step = blockDim.x;
-    for (int base = threadIdx.x; base < NE; base += step * U) {
-        int4 v[U];
-        int jd[U];
+    const uint32_t* tab = halo_table<E>();
+    for (int j = threadIdx.x; j < NC; j += BS) cp_async16(&cell[j], own + j);
+    int4 v[U];
+    int jd[U];
+    auto fetch = [&](int base) {
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            int e = base + u * step;
+            int e = base + u * BS;
             jd[u] = -1;
             v[u] = make_int4(0, 0, 0, 0);
             if (e < NE) {
-                int d, j, jj;
-                halo_entry<E>(e, d, j, jj);
-                int t = nbr[d];
+                uint32_t w = __ldg(tab + e);
+                int t = nbr[w & 31u];
                 if (t >= 0) {
-                    v[u] = __ldg(tiles + (size_t)t * NC + jj);
-                    jd[u] = j;
+                    v[u] = __ldg(tiles + (size_t)t * NC + (w >> 18));
+                    jd[u] = (int)((w >> 5) & 0x1fffu);
                 }
             }
         }
+    };
+    auto add = [&]() {
 #pragma unroll
         for (int u = 0; u < U; u++) {
             if (jd[u] >= 0) {
@@ -870,18 +885,30 @@ __device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr,
                 atomicAdd(dst + 3, v[u].w);
             }
         }
+    };
+    fetch(threadIdx.x);
+    cp_async_wait_all();
+    __syncthreads();
+    if (COPY_MASS) {
+        for (int j = threadIdx.x; j < NC; j += BS) own_mass[j] = (uint32_t)cell[j].x;
+        __syncthreads();
+    }
+    add();
+    for (int base = threadIdx.x + U * BS; base < NE; base += U * BS) {
+        fetch(base);
+        add();
     }
 }
 
 // Assemble this tile's (E+2)^3 cell velocities in shared memory: halo sums
 // (assemble_sums), then each sum turned into the velocity in place.
-template <int E, bool PB, bool COPY_MASS = false>
+template <int E, int BS, bool PB, bool COPY_MASS = false>
 __device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
                                                        const int* nbr, int4* cell, uint32_t* own_mass = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
-    assemble_sums<E, 8, COPY_MASS>(tiles, nbr, cell, own_mass);
+    assemble_sums<E, BS, COPY_MASS>(tiles, nbr, cell, own_mass);
     __syncthreads();
-    for (int j = threadIdx.x; j < NC; j += blockDim.x) {
+    for (int j = threadIdx.x; j < NC; j += BS) {
         int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
         int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
         float4 v = cell_velocity<PB>(S, cell[j], gc);
@@ -1104,6 +1131,30 @@ __device__ __forceinline__ uint32_t n_tiles_now(const Ctx& c) {
     return n < c.max_tiles ? n : c.max_tiles;
 }
 
+// Neighbour table of the compact tiles, once per substep: entry st*27 + d is
+// the compact index of the tile at offset d = 9(dz+1) + 3(dy+1) + (dx+1), or
+// -1 when that tile is unoccupied or past the tile storage.
+template <int E>
+__global__ void __launch_bounds__(256) k_tile_nbr(Ctx c) {
+    uint32_t n = n_tiles_now(c) * 27u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t st = i / 27u, d = i - st * 27u;
+        int r = (int)st;
+        if (d != 13u) {
+            uint32_t scene;
+            int sx, sy, sz;
+            unpack_key(c.st_key[st], scene, sx, sy, sz);
+            sx += (int)(d % 3u) - 1;
+            sy += (int)((d / 3u) % 3u) - 1;
+            sz += (int)(d / 9u) - 1;
+            uint32_t slot = tile_lookup(c, pack_key(scene, sx, sy, sz), scene, sx, sy, sz);
+            r = (slot == INVALID) ? -1 : (int)c.slot_st[slot];
+            if (r >= (int)c.max_tiles) r = -1;
+        }
+        c.st_nbr[i] = r;
+    }
+}
+
 // ------------------------------------------------------------------
 // explicit P2G (particleToGrid.cs.wgsl:27-79)
 // ------------------------------------------------------------------
@@ -1192,10 +1243,9 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
     for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
+        load_neighbors(c, st, nbr);
         __syncthreads();
-        lookup_neighbors<E>(c, T, st, nbr);
-        __syncthreads();
-        assemble_velocity_tile<E, PB>(c.tiles_b, S, T, nbr, cell);
+        assemble_velocity_tile<E, BS, PB>(c.tiles_b, S, T, nbr, cell);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1294,11 +1344,10 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
-        __syncthreads();
-        lookup_neighbors<E>(c, T, st, nbr);
+        load_neighbors(c, st, nbr);
         zero_mom<E>(acc);
         __syncthreads();
-        assemble_velocity_tile<E, true, true>(c.tiles_b, S, T, nbr, cell, acc);
+        assemble_velocity_tile<E, BS, true, true>(c.tiles_b, S, T, nbr, cell, acc);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1333,7 +1382,7 @@ __global__ void __launch_bounds__(256) k_grid_dense(Ctx c, uint32_t scene, int a
         tile_begin<E>(c, st, S, T, cur_scene);
         __syncthreads();
         if (T.scene != scene) continue;
-        lookup_neighbors<E>(c, T, st, nbr);
+        load_neighbors(c, st, nbr);
         __syncthreads();
         for (int j = threadIdx.x; j < NC; j += blockDim.x) {
             int4 s = assemble_cell<E>(c.tiles_b, nbr, j);
@@ -1441,6 +1490,7 @@ void* kernel_ptr(uint32_t kid) {
         case K_PBMPM_ITER: return (void*)k_pbmpm_iter<E, iter_block<E>()>;
         case K_G2P_PBMPM: return (void*)k_g2p_integrate<E, true, BS_DEFAULT>;
         case K_GRID_DENSE: return (void*)k_grid_dense<E>;
+        case K_TILE_NBR: return (void*)k_tile_nbr<E>;
         default: return nullptr;
     }
 }
@@ -1473,6 +1523,7 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
         case K_COMPACT_B: k_compact_b<<<1, 1024, 0, s>>>(c, n_chunks); break;
         case K_COMPACT_C: k_compact_c<<<n_chunks, 256, 0, s>>>(c); break;
         case K_BIN_SCATTER: if (pblocks) k_bin_scatter<<<pblocks, 256, 0, s>>>(c); break;
+        case K_TILE_NBR: k_tile_nbr<E><<<grid_tiles, 256, 0, s>>>(c); break;
         case K_P2G_EXPLICIT: k_p2g_explicit<E, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
         case K_G2P_EXPLICIT: k_g2p_integrate<E, false, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
         case K_PBMPM_FIRST: k_pbmpm_first<E, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
