@@ -50,6 +50,7 @@ extern "C" {
 #define MPM_STATUS_BVH_STACK      0x4u  /* BVH traversal dropped children (stack of 32 full) */
 #define MPM_STATUS_SCENE_RANGE    0x8u  /* a particle index belongs to no scene */
 #define MPM_STATUS_MLP_FALLBACK   0x10u /* learned plasticity fell back to the exact map */
+#define MPM_STATUS_MLP_TIMEOUT    0x20u /* a tensor-core wait of the plasticity pass ran out */
 
 typedef struct MpmHandle MpmHandle;
 
@@ -171,6 +172,93 @@ int mpm_use_graphs(MpmHandle* h, int enable);
  * a NaN. */
 int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* ident_mismatches, uint64_t* cvt_mismatches,
                  uint64_t* nan_conversion);
+
+/* ---- learned plasticity --------------------------------------------
+ * The snow return map applyPlasticity (src/lib/gpu/shaderPrelude/
+ * plasticityOps.wgsl:7-48, called from integrateParticles.wgsl) can run in
+ * four ways, chosen per handle:
+ *   INLINE  (default) the exact map inside the integrate kernel, as the reference;
+ *   EXACT   integrate applies a strain-bound check (all Gershgorin discs of
+ *           Fe^T Fe inside the elastic band, so the exact map would return
+ *           its input unchanged) and lists the rest; a separate pass runs
+ *           the exact map on them.  Results equal INLINE bit for bit;
+ *   COLLECT as EXACT, and each listed particle inside the trained domain
+ *           also writes a training pair (12 inputs, 10 targets) to the
+ *           buffer given by mpm_set_pair_buffer;
+ *   LEARNED as EXACT, but the pass runs the network (BF16 tensor cores,
+ *           FP32 accumulation) and takes its answer unless the particle is
+ *           outside the trained domain, the uncertainty output exceeds
+ *           unc_threshold, or the determinant check fails (|ln det Fp'
+ *           recomputed - ln J_p predicted| > det_threshold); those particles,
+ *           and an audited fraction of the rest, take the exact map.
+ * Network: 12 -> 64 -> 64 -> 64 -> 11, SiLU.  Inputs: (Fe_trial - I) * 20
+ * (9, column-major), 2 ln det Fp, log2(dt) + 13.2877, (theta_c - 0.025) * 100.
+ * Targets: (Fe' - Fe_trial) * 100 (9), (ln det Fp' - ln det Fp) * 100; output
+ * 10 estimates the error norm of the other ten.  Parameters: MPM_MLP_PARAMS
+ * FP32 values packed [W1 64x12 | b1 64 | W2 64x64 | b2 | W3 64x64 | b3 |
+ * W4 11x64 | b4 11], W row-major [out][in].  No counterpart in the reference
+ * (its plasticity is always the exact map). */
+#define MPM_PLASTICITY_INLINE 0
+#define MPM_PLASTICITY_EXACT 1
+#define MPM_PLASTICITY_COLLECT 2
+#define MPM_PLASTICITY_LEARNED 3
+#define MPM_MLP_INPUTS 12
+#define MPM_MLP_HIDDEN 64
+#define MPM_MLP_OUTPUTS 11
+#define MPM_MLP_TARGETS 10
+#define MPM_MLP_PARAMS 9867
+
+typedef struct MpmMlp MpmMlp;
+
+typedef struct MpmMlpTrainConfig {
+    uint32_t epochs;
+    uint32_t batch;        /* pairs per Adam step */
+    float lr;              /* initial learning rate, cosine-decayed to lr_final */
+    float lr_final;
+    float unc_weight;      /* weight of the uncertainty head's loss */
+    uint32_t seed;         /* shuffling */
+} MpmMlpTrainConfig;
+
+typedef struct MpmPlasticityStats {
+    uint64_t candidates;          /* particles the strain-bound check did not clear */
+    uint64_t learned;             /* took the network's answer */
+    uint64_t fallback_domain;     /* exact: outside the trained domain */
+    uint64_t fallback_uncertain;  /* exact: uncertainty above threshold */
+    uint64_t fallback_det;        /* exact: determinant check failed */
+    uint64_t audited;             /* exact, with the network's error recorded */
+    float audit_max_err;          /* max over audited particles of max |Fe'_net - Fe'_exact| */
+    float audit_mean_err;
+    uint32_t pairs_collected;
+    uint32_t pad;
+} MpmPlasticityStats;
+
+/* Seeded initial parameters (host only). */
+int mpm_mlp_init_params(uint32_t seed, float* out);
+int mpm_mlp_create(int device, uint32_t seed, MpmMlp** out);
+int mpm_mlp_destroy(MpmMlp* m);
+const char* mpm_mlp_last_error(const MpmMlp* m);
+int mpm_mlp_get_params(MpmMlp* m, float* host_out);
+int mpm_mlp_set_params(MpmMlp* m, const float* host_in);
+/* Network outputs for n inputs (device arrays [n][12] -> [n][11]); synchronous. */
+int mpm_mlp_forward(MpmMlp* m, const float* x_dev, uint32_t n, float* y_dev);
+/* Loss and gradient of the batch loss over n pairs (device arrays
+ * [n][12], [n][10]) at the current parameters; grad_host receives
+ * MPM_MLP_PARAMS values.  Loss = (1/n) sum [ |y[0..9] - t|^2 +
+ * unc_weight (y[10] - |y[0..9] - t|)^2 ]. */
+int mpm_mlp_gradient(MpmMlp* m, const float* x_dev, const float* t_dev, uint32_t n, float unc_weight,
+                     float* grad_host, float* loss_host);
+/* Adam training on the GPU over n pairs; loss_per_epoch (may be NULL)
+ * receives cfg->epochs mean batch losses. */
+int mpm_mlp_train(MpmMlp* m, const float* x_dev, const float* t_dev, uint32_t n,
+                  const MpmMlpTrainConfig* cfg, float* loss_per_epoch);
+/* Selects the plasticity mode of a handle (net: required for LEARNED, must
+ * outlive its use and must not train while the handle steps). */
+int mpm_set_plasticity(MpmHandle* h, int mode, MpmMlp* net, float unc_threshold, float det_threshold,
+                       float audit_fraction);
+/* Training-pair buffer for COLLECT mode (device arrays [capacity][12],
+ * [capacity][10]); resets the pair count. */
+int mpm_set_pair_buffer(MpmHandle* h, float* x_dev, float* t_dev, uint32_t capacity);
+int mpm_get_plasticity_stats(MpmHandle* h, MpmPlasticityStats* out, int reset);
 
 /* ---- allocation-free substep ----------------------------------------
  * No counterpart in the reference (its TypeScript managers own every GPU

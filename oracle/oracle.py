@@ -21,7 +21,7 @@ UNIFORMS_BYTES = 37376
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "mlp_oracle.c", "Makefile")]
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return LIB
@@ -68,6 +68,11 @@ def lib():
             "orf_inverse": (None, [V, V]), "orf_polar": (None, [V, V]), "orf_det": (C.c_float, [V]),
             "orf_plasticity": (None, [V, V, V]),
             "or_bvh_build": (U32, [V, U32, V, U32, V, V]),
+            "or_mlp_forward": (None, [V, V, U32, I32, V]),
+            "or_mlp_gradient": (C.c_double, [V, V, V, U32, C.c_float, I32, V]),
+            "or_mlp_features": (I32, [V, V, C.c_float, C.c_float, V]),
+            "or_mlp_targets": (None, [V, V, V, V, V]),
+            "or_cert_elastic": (I32, [C.c_float, C.c_float, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -183,3 +188,47 @@ def aggregates(pos, vel, mass, Fp9):
     mom = (vel * m[:, None]).sum(0)
     jp = np.linalg.det(F).mean()
     return com, mom, jp
+
+
+# ---- learned-plasticity network checker (mlp_oracle.c) ----------------
+MLP_PARAMS = 9867
+
+
+def mlp_forward(params, x, bf16=True):
+    """Network outputs [n, 11] (f64) of inputs x [n, 12]."""
+    p = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    y = np.zeros((xx.shape[0], 11), np.float64)
+    lib().or_mlp_forward(p.ctypes.data, xx.ctypes.data, xx.shape[0], 1 if bf16 else 0, y.ctypes.data)
+    return y
+
+
+def mlp_gradient(params, x, t, unc_weight=0.1, bf16=True):
+    """(loss, gradient [MLP_PARAMS] f64) of the batch loss."""
+    p = np.ascontiguousarray(params, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    tt = np.ascontiguousarray(t, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float64)
+    loss = lib().or_mlp_gradient(p.ctypes.data, xx.ctypes.data, tt.ctypes.data, xx.shape[0], unc_weight,
+                                 1 if bf16 else 0, g.ctypes.data)
+    return loss, g
+
+
+def mlp_pair(Fe, Fp, dt, theta_c, theta_s):
+    """(in_domain, x[12], t[10], Fe', Fp') of one trial state through the exact map."""
+    fe = np.ascontiguousarray(Fe, np.float32).reshape(9)
+    fp = np.ascontiguousarray(Fp, np.float32).reshape(9)
+    x = np.zeros(12, np.float32)
+    ok = lib().or_mlp_features(fe.ctypes.data, fp.ctypes.data, dt, theta_c, x.ctypes.data)
+    e = make_ext({"theta_c": theta_c, "theta_s": theta_s})
+    fe2, fp2 = fe.copy(), fp.copy()
+    lib().orf_plasticity(C.byref(e), fe2.ctypes.data, fp2.ctypes.data)
+    t = np.zeros(10, np.float32)
+    lib().or_mlp_targets(fe.ctypes.data, fp.ctypes.data, fe2.ctypes.data, fp2.ctypes.data, t.ctypes.data)
+    return bool(ok), x, t, fe2, fp2
+
+
+def cert_elastic(Fe, theta_c, theta_s):
+    fe = np.ascontiguousarray(Fe, np.float32).reshape(9)
+    smin, smax = np.float32(1.0 - float(np.float32(theta_c))), np.float32(1.0 + float(np.float32(theta_s)))
+    return bool(lib().or_cert_elastic(float(smin), float(smax), fe.ctypes.data))

@@ -1,0 +1,179 @@
+"""Learned plasticity on the GPU: the tensor-core network against the CPU
+checker (forward pass and gradients), the deferred exact pass against the
+inline exact map (bit for bit), the collected training pairs against the
+exact return map, and the trained surrogate in a substep (accuracy of the
+aggregates against the f64 oracle, and what the trained network gains over
+an untrained one)."""
+import numpy as np
+import pytest
+
+from helpers import GpuScene, compare_states, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _net(gpu, seed=0):
+    return gpu.learned.PlasticityNet(device=0, seed=seed)
+
+
+def test_network_forward_matches_oracle(gpu, oracle_mod):
+    torch = _torch()
+    rng = np.random.default_rng(0)
+    net = _net(gpu, seed=3)
+    P = rng.normal(0, 0.15, oracle_mod.MLP_PARAMS).astype(np.float32)
+    net.params = P
+    x = rng.normal(0, 1, (1000, 12)).astype(np.float32)      # 7 full tiles and a ragged one
+    y = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    want = oracle_mod.mlp_forward(P, x, bf16=True)
+    # FP32 tensor-core accumulation vs f64, plus rare one-ulp BF16 rounding flips
+    assert np.all(np.abs(y - want) <= 3e-3 + 1e-2 * np.abs(want)), np.max(np.abs(y - want))
+    assert np.mean(np.abs(y - want)) < 2e-4
+    net.close()
+
+
+def test_network_gradient_matches_oracle(gpu, oracle_mod):
+    torch = _torch()
+    rng = np.random.default_rng(1)
+    net = _net(gpu)
+    P = rng.normal(0, 0.15, oracle_mod.MLP_PARAMS).astype(np.float32)
+    net.params = P
+    n = 300
+    x = rng.normal(0, 1, (n, 12)).astype(np.float32)
+    t = rng.normal(0, 1, (n, 10)).astype(np.float32)
+    loss, g = net.gradient(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), unc_weight=0.25)
+    want_loss, want = oracle_mod.mlp_gradient(P, x, t, 0.25, bf16=True)
+    assert abs(loss - want_loss) <= 1e-3 * abs(want_loss)
+    # per tensor: W1 b1 W2 b2 W3 b3 W4 b4
+    bounds = [0, 768, 832, 4928, 4992, 9088, 9152, 9856, 9867]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        err = np.linalg.norm(g[a:b] - want[a:b]) / (np.linalg.norm(want[a:b]) + 1e-12)
+        assert err < 2e-2, (a, b, err)
+    net.close()
+
+
+def _scene(gpu, kind, seed=10, n_side=16):
+    return gpu.scenes.parity_scene(kind=kind, n_side=n_side, seed=seed, with_collider=True)
+
+
+@pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
+def test_deferred_exact_equals_inline(gpu, kind):
+    """The strain-bound check plus a separate exact pass reproduces the
+    inline exact map bit for bit, over several substeps with yielding."""
+    spec = _scene(gpu, kind)
+    a = GpuScene(gpu, spec)
+    b = GpuScene(gpu, spec)
+    ctl = gpu.learned.PlasticityController(b.buf)
+    ctl.set_mode(gpu._lib.PLASTICITY_EXACT)
+    assert a.step(6) == 0 and b.step(6) == 0
+    compare_states(b.particles(), a.particles())
+    st = ctl.stats()
+    assert st["candidates"] == 0   # exact mode runs no network and counts nothing
+    a.close()
+    b.close()
+
+
+def _collect(gpu, specs, steps, cap):
+    """Rollouts in COLLECT mode; returns the pairs (x, t) on the device."""
+    torch = _torch()
+    xs, ts = [], []
+    for spec in specs:
+        g = GpuScene(gpu, spec)
+        ctl = gpu.learned.PlasticityController(g.buf)
+        ctl.set_mode(gpu._lib.PLASTICITY_COLLECT)
+        x, t = ctl.collect_into(cap)
+        assert g.step(steps) == 0
+        n = ctl.stats()["pairs_collected"]
+        xs.append(x[:n].clone())
+        ts.append(t[:n].clone())
+        g.close()
+    return torch.cat(xs), torch.cat(ts)
+
+
+def test_collected_pairs_match_exact_map(gpu, oracle_mod):
+    spec = _scene(gpu, "explicit", seed=11)
+    # the collecting run itself follows the exact map: same states as inline
+    a = GpuScene(gpu, spec)
+    b = GpuScene(gpu, spec)
+    ctl = gpu.learned.PlasticityController(b.buf)
+    ctl.set_mode(gpu._lib.PLASTICITY_COLLECT)
+    x, t = ctl.collect_into(200000)
+    assert a.step(3) == 0 and b.step(3) == 0
+    compare_states(b.particles(), a.particles())
+    n = ctl.stats()["pairs_collected"]
+    assert n > 500
+    xh, th = x[:n].cpu().numpy(), t[:n].cpu().numpy()
+    assert np.any(np.abs(th) > 0), "no yielding pair"
+    # each pair's target against the exact map of the oracle on the decoded input
+    # (decoding (x / 20) + I rounds; states within 1e-5 of the band edge may flip)
+    rng = np.random.default_rng(0)
+    bad = 0
+    pick = rng.choice(n, min(n, 400), replace=False)
+    dt = float(np.frombuffer(spec.uniforms.bytes()[0:4], "<f4")[0])
+    for i in pick:
+        Fe = (xh[i, :9] / np.float32(20.0) + np.eye(3, dtype=np.float32).reshape(9)).astype(np.float32)
+        jp = np.exp(xh[i, 9] / 2.0)
+        Fp = (np.eye(3) * jp ** (1.0 / 3.0)).astype(np.float32).reshape(9)
+        ok, xo, to, _, _ = oracle_mod.mlp_pair(Fe, Fp, dt, 0.025, 7.5e-3)
+        assert ok
+        if not np.allclose(th[i, :9], to[:9], atol=2e-3):
+            bad += 1
+    assert bad <= 0.02 * len(pick), bad
+
+
+def _aggregates(oracle_mod, rec):
+    return oracle_mod.aggregates(rec["pos"], rec["vel"], rec["mass"], rec["Fp"][:, :, :3].reshape(-1, 9))
+
+
+def _agg_close(a, b):
+    com = np.allclose(a[0], b[0], rtol=1e-3, atol=1e-3)
+    mom = np.allclose(a[1], b[1], rtol=1e-3, atol=1e-3 * np.abs(b[1]).max() + 1e-12)
+    jp = abs(a[2] - b[2]) <= 1e-3 * abs(b[2])
+    return com and mom and jp
+
+
+def test_trained_network_gains_over_untrained(gpu, oracle_mod):
+    """Trains the network on pairs the exact map generated in rollouts, then
+    runs a held-out scene with the learned map.  The trained network answers
+    most of the particles the strain-bound check sends to it, its audited
+    error is a small fraction of an untrained network's, and the aggregates
+    (centre of mass, momentum, mean J_p) stay within 1e-3 of the f64 oracle,
+    as the inline exact map's do."""
+    kind = "explicit"
+    specs = [_scene(gpu, kind, seed=s) for s in (21, 22, 23, 24, 25, 26)]
+    x, t = _collect(gpu, specs, 20, 400000)
+    assert x.shape[0] > 10000, x.shape
+    net = _net(gpu, seed=5)
+    untrained = net.params.copy()
+    hist = net.train(x, t, epochs=60, batch=1024, lr=3e-3, lr_final=3e-5, unc_weight=0.1, seed=1)
+    assert hist[-1] < 0.05 * hist[0], hist
+    spec = _scene(gpu, kind, seed=31)
+    n_steps = 12
+    runs = {}
+    for name, params in (("trained", net.params.copy()), ("untrained", untrained)):
+        net.params = params
+        g = GpuScene(gpu, spec)
+        ctl = gpu.learned.PlasticityController(g.buf)
+        ctl.set_mode(gpu._lib.PLASTICITY_LEARNED, net, unc_threshold=0.2, det_threshold=1e-3, audit_fraction=0.05)
+        assert g.step(n_steps) == 0
+        runs[name] = (g.particles(), ctl.stats())
+        g.close()
+    plain = GpuScene(gpu, spec)
+    assert plain.step(n_steps) == 0
+    exact = plain.particles()
+    plain.close()
+    got, st = runs["trained"]
+    st0 = runs["untrained"][1]
+    assert st["candidates"] > 1000, st
+    assert st["learned"] > 0.5 * st["candidates"], st
+    assert st["audited"] > 0 and st0["audited"] > 0, (st, st0)
+    assert st["audit_mean_err"] < 0.2 * st0["audit_mean_err"], (st, st0)
+    _, w64 = run_oracle(oracle_mod, spec, n_steps=n_steps, fp64=True)
+    a64 = oracle_mod.aggregates(w64["pos"], w64["vel"], w64["mass"], w64["Fp"])
+    assert _agg_close(_aggregates(oracle_mod, exact), a64)
+    assert _agg_close(_aggregates(oracle_mod, got), a64)
+    net.close()

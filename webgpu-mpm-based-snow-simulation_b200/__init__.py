@@ -6,7 +6,7 @@ records come out.  Compute runs in libmpm.so (include/mpm.h); this package is
 the host-side mirror of the reference's TypeScript managers plus scene
 generators.
 """
-from . import _lib, layout, scenes
+from . import _lib, layout, learned, scenes
 from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams, default_params, load
 from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
 from .pipeline import (GpuColliderBufferManager, GpuMpmBufferManager, GpuMpmPipelineManager,
@@ -16,5 +16,5 @@ __all__ = [
     "METHOD_EXPLICIT", "METHOD_PBMPM", "MpmConfig", "MpmError", "MpmParams", "default_params", "load",
     "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
     "GpuMpmBufferManager", "GpuMpmPipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
-    "layout", "scenes",
+    "layout", "scenes", "learned",
 ]

@@ -21,7 +21,17 @@ STATUS_BITS = {
     0x4: "BVH stack overflow",
     0x8: "particle outside every scene range",
     0x10: "learned plasticity fallback",
+    0x20: "learned plasticity tensor-core wait ran out",
 }
+
+PLASTICITY_INLINE = 0
+PLASTICITY_EXACT = 1
+PLASTICITY_COLLECT = 2
+PLASTICITY_LEARNED = 3
+MLP_INPUTS = 12
+MLP_OUTPUTS = 11
+MLP_TARGETS = 10
+MLP_PARAMS = 9867
 
 
 class MpmConfig(C.Structure):
@@ -69,6 +79,21 @@ class MpmParams(C.Structure):
         return d
 
 
+class MpmMlpTrainConfig(C.Structure):
+    _fields_ = [("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float), ("lr_final", C.c_float),
+                ("unc_weight", C.c_float), ("seed", C.c_uint32)]
+
+
+class MpmPlasticityStats(C.Structure):
+    _fields_ = [("candidates", C.c_uint64), ("learned", C.c_uint64), ("fallback_domain", C.c_uint64),
+                ("fallback_uncertain", C.c_uint64), ("fallback_det", C.c_uint64), ("audited", C.c_uint64),
+                ("audit_max_err", C.c_float), ("audit_mean_err", C.c_float), ("pairs_collected", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
+
+
 # exported symbols and their signatures: (restype, argtypes)
 _H = C.c_void_p
 SIGNATURES = {
@@ -102,6 +127,20 @@ SIGNATURES = {
     "mpm_use_graphs": (C.c_int, [_H, C.c_int]),
     "mpm_selftest": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                C.POINTER(C.c_uint64)]),
+    "mpm_mlp_init_params": (C.c_int, [C.c_uint32, C.c_void_p]),
+    "mpm_mlp_create": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "mpm_mlp_destroy": (C.c_int, [C.c_void_p]),
+    "mpm_mlp_last_error": (C.c_char_p, [C.c_void_p]),
+    "mpm_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mpm_mlp_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mpm_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "mpm_mlp_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p,
+                                   C.c_void_p]),
+    "mpm_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(MpmMlpTrainConfig),
+                                C.c_void_p]),
+    "mpm_set_plasticity": (C.c_int, [_H, C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_float]),
+    "mpm_set_pair_buffer": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "mpm_get_plasticity_stats": (C.c_int, [_H, C.POINTER(MpmPlasticityStats), C.c_int]),
     "mpm_step_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_size_t,
                                    C.POINTER(MpmParams), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p, C.c_uint32,
                                    C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]),

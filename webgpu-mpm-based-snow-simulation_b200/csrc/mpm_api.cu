@@ -19,6 +19,7 @@
 #include "../../include/mpm.h"
 #include "mpm_engine.cuh"
 #include "mpm_math.cuh"
+#include "mpm_mlp.cuh"
 
 namespace mpm {
 template <int E> cudaError_t configure_tile_kernels(int* blocks_per_sm);
@@ -32,7 +33,7 @@ using namespace mpm;
 static const char* kKernelNames[K_COUNT] = {
     "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
     "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense",
-    "tile_nbr"};
+    "tile_nbr", "plasticity"};
 
 struct TimedLaunch {
     uint32_t kid;
@@ -46,6 +47,22 @@ struct SceneHost {
     bool have_uniforms = false;
     uint32_t* col_data = nullptr;
     uint32_t* bvh = nullptr;
+};
+
+struct MpmMlp {
+    int device = 0;
+    int n_sms = 0;
+    cudaStream_t stream = nullptr;
+    float* params = nullptr;   // NPARAM FP32 masters
+    float* adam_m = nullptr;
+    float* adam_v = nullptr;
+    float* grad = nullptr;
+    float* loss = nullptr;     // [2]: batch loss accumulator, epoch accumulator
+    uint32_t* err = nullptr;
+    uint32_t* idx = nullptr;   // shuffled pair order of one epoch
+    uint32_t idx_cap = 0;
+    int adam_step = 0;
+    std::string msg;
 };
 
 struct MpmHandle {
@@ -82,6 +99,17 @@ struct MpmHandle {
     uint32_t* chunk_np = nullptr;
     int4* tiles[2] = {nullptr, nullptr};
     int32_t* st_nbr = nullptr;    // max_tiles x 27 neighbour indices
+    // deferred / learned plasticity
+    int plast_mode = PLAST_INLINE;
+    MpmMlp* mlp = nullptr;
+    float unc_threshold = 0.05f, det_threshold = 1e-3f;
+    uint32_t audit_threshold = 0;
+    uint32_t* plast_list = nullptr;   // max_particles
+    PlastStats* d_stats = nullptr;
+    float* pair_x = nullptr;
+    float* pair_t = nullptr;
+    uint32_t* d_pair_count = nullptr;
+    uint32_t pair_cap = 0;
     float4* iter_rec = nullptr;   // PBMPM iteration records, IR_PLANES x N float4
     int last_tiles = 0;
     SceneDev* d_scenes = nullptr;
@@ -288,7 +316,8 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     for (auto e : h->event_pool) cudaEventDestroy(e);
     void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
-                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters, h->iter_rec, h->st_nbr};
+                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters, h->iter_rec, h->st_nbr,
+                    h->plast_list, h->d_stats, h->d_pair_count};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h->own_particles && h->particles) cudaFree(h->particles);
@@ -384,6 +413,10 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     CK(h, cudaMalloc(&h->d_scene_first, (size_t)(max_scenes + 1) * 4));
     CK(h, cudaMalloc(&h->counters, sizeof(Counters)));
     CK(h, cudaMemsetAsync(h->counters, 0, sizeof(Counters), h->stream));
+    CK(h, cudaMalloc(&h->d_stats, sizeof(PlastStats)));
+    CK(h, cudaMemsetAsync(h->d_stats, 0, sizeof(PlastStats), h->stream));
+    CK(h, cudaMalloc(&h->d_pair_count, 4));
+    CK(h, cudaMemsetAsync(h->d_pair_count, 0, 4, h->stream));
     {
         int r = alloc_table(h, h->cap);
         if (r) return r;
@@ -604,6 +637,8 @@ static Ctx make_ctx(MpmHandle* h, int parity) {
     c.tiles_b = h->tiles[0];
     c.iter_rec = h->iter_rec;
     c.st_nbr = h->st_nbr;
+    c.plast_list = h->plast_list;
+    c.plast_defer = h->plast_mode != PLAST_INLINE ? 1u : 0u;
     c.scenes = h->d_scenes;
     c.scene_first = h->d_scene_first;
     c.counters = h->counters;
@@ -649,7 +684,22 @@ static cudaError_t launch(MpmHandle* h, uint32_t kid, const Ctx& c, bool capturi
         tl.b = get_event(h);
         cudaEventRecord(tl.a, h->stream);
     }
-    cudaError_t e = launch_e(h->tile_edge, kid, c, h->stream, grid, 0, 0, nullptr);
+    cudaError_t e;
+    if (kid == K_PLASTICITY) {
+        PlastCtx pc{};
+        pc.params = h->mlp ? h->mlp->params : nullptr;
+        pc.unc_threshold = h->unc_threshold;
+        pc.det_threshold = h->det_threshold;
+        pc.audit_threshold = h->audit_threshold;
+        pc.stats = h->d_stats;
+        pc.pair_x = h->pair_x;
+        pc.pair_t = h->pair_t;
+        pc.pair_count = h->d_pair_count;
+        pc.pair_cap = h->pair_cap;
+        e = launch_plasticity(h->plast_mode, c, pc, h->n_sms * (h->plast_mode == PLAST_LEARNED ? 4 : 8), h->stream);
+    } else {
+        e = launch_e(h->tile_edge, kid, c, h->stream, grid, 0, 0, nullptr);
+    }
     if (timed) {
         cudaEventRecord(tl.b, h->stream);
         h->pending.push_back(tl);
@@ -681,6 +731,7 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
         if (stop_p2g) { h->last_tiles = 0; return cudaSuccess; }
         c.tiles_b = h->tiles[0];
         L(K_G2P_EXPLICIT);
+        if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = 0;
     } else {
         uint32_t n_iter = h->scenes[0].params.n_iter;
@@ -696,6 +747,7 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
         }
         c.tiles_b = h->tiles[cur];
         L(K_G2P_PBMPM);
+        if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = cur;
     }
 #undef L
@@ -773,6 +825,12 @@ static uint64_t graph_signature(MpmHandle* h) {
     s = s * 1315423911ull + h->n_scenes;
     s = s * 1315423911ull + h->scenes[0].params.n_iter;
     s = s * 1315423911ull + (uint64_t)(uintptr_t)h->particles;
+    s = s * 1315423911ull + (uint64_t)h->plast_mode;
+    s = s * 1315423911ull + (uint64_t)(uintptr_t)(h->mlp ? h->mlp->params : nullptr);
+    s = s * 1315423911ull + (uint64_t)(uintptr_t)h->pair_x + h->pair_cap;
+    s = s * 1315423911ull + (uint64_t)h->audit_threshold + (uint64_t)__builtin_bit_cast(uint32_t, h->unc_threshold) +
+        ((uint64_t)__builtin_bit_cast(uint32_t, h->det_threshold) << 32);
+    s = s * 1315423911ull + (uint64_t)(uintptr_t)h->plast_list;
     return s | 1ull;
 }
 
@@ -948,6 +1006,246 @@ extern "C" int mpm_use_graphs(MpmHandle* h, int enable) {
     if (!h) return MPM_ERR_ARG;
     h->use_graphs = enable != 0;
     if (!h->use_graphs) destroy_graphs(h);
+    return MPM_OK;
+}
+
+// ---------------------------------------------------------------------
+// Learned plasticity: the network object, its training, and its use by a handle
+// ---------------------------------------------------------------------
+static int mlp_fail(MpmMlp* m, int code, const char* fmt, ...) {
+    if (m) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        m->msg = buf;
+    }
+    return code;
+}
+#define MCK(m, expr)                                                                              \
+    do {                                                                                          \
+        cudaError_t _e = (expr);                                                                  \
+        if (_e != cudaSuccess) return mlp_fail((m), MPM_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+static uint64_t splitmix(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Glorot-uniform weights, zero biases; the last layer starts at a tenth of that
+extern "C" int mpm_mlp_init_params(uint32_t seed, float* out) {
+    if (!out) return MPM_ERR_ARG;
+    uint64_t st = 0x6d6c70ull ^ ((uint64_t)seed << 20);
+    std::memset(out, 0, sizeof(float) * mlp::NPARAM);
+    struct L { int ow, out, in; float gain; } layers[4] = {{mlp::OW1, mlp::HID, mlp::IN, 1.f},
+                                                          {mlp::OW2, mlp::HID, mlp::HID, 1.f},
+                                                          {mlp::OW3, mlp::HID, mlp::HID, 1.f},
+                                                          {mlp::OW4, mlp::OUT, mlp::HID, 0.1f}};
+    for (auto& l : layers) {
+        float a = l.gain * std::sqrt(6.0f / (float)(l.in + l.out));
+        for (int i = 0; i < l.out * l.in; i++) {
+            double u = (double)(splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
+            out[l.ow + i] = (float)((2.0 * u - 1.0) * a);
+        }
+    }
+    return MPM_OK;
+}
+
+extern "C" int mpm_mlp_create(int device, uint32_t seed, MpmMlp** out) {
+    if (!out) return MPM_ERR_ARG;
+    MpmMlp* m = new MpmMlp();
+    *out = m;
+    m->device = device;
+    MCK(m, cudaSetDevice(device));
+    MCK(m, cudaDeviceGetAttribute(&m->n_sms, cudaDevAttrMultiProcessorCount, device));
+    MCK(m, cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    MCK(m, cudaMalloc(&m->params, mlp::NPARAM * 4));
+    MCK(m, cudaMalloc(&m->adam_m, mlp::NPARAM * 4));
+    MCK(m, cudaMalloc(&m->adam_v, mlp::NPARAM * 4));
+    MCK(m, cudaMalloc(&m->grad, mlp::NPARAM * 4));
+    MCK(m, cudaMalloc(&m->loss, 8));
+    MCK(m, cudaMalloc(&m->err, 4));
+    MCK(m, cudaMemset(m->adam_m, 0, mlp::NPARAM * 4));
+    MCK(m, cudaMemset(m->adam_v, 0, mlp::NPARAM * 4));
+    MCK(m, cudaMemset(m->err, 0, 4));
+    MCK(m, configure_mlp_kernels());
+    std::vector<float> p(mlp::NPARAM);
+    mpm_mlp_init_params(seed, p.data());
+    MCK(m, cudaMemcpy(m->params, p.data(), mlp::NPARAM * 4, cudaMemcpyHostToDevice));
+    return MPM_OK;
+}
+
+extern "C" int mpm_mlp_destroy(MpmMlp* m) {
+    if (!m) return MPM_ERR_ARG;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    void* bufs[] = {m->params, m->adam_m, m->adam_v, m->grad, m->loss, m->err, m->idx};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return MPM_OK;
+}
+
+extern "C" const char* mpm_mlp_last_error(const MpmMlp* m) { return m ? m->msg.c_str() : "null network"; }
+
+extern "C" int mpm_mlp_get_params(MpmMlp* m, float* host_out) {
+    if (!m || !host_out) return MPM_ERR_ARG;
+    cudaSetDevice(m->device);
+    MCK(m, cudaStreamSynchronize(m->stream));
+    MCK(m, cudaMemcpy(host_out, m->params, mlp::NPARAM * 4, cudaMemcpyDeviceToHost));
+    return MPM_OK;
+}
+
+extern "C" int mpm_mlp_set_params(MpmMlp* m, const float* host_in) {
+    if (!m || !host_in) return MPM_ERR_ARG;
+    cudaSetDevice(m->device);
+    MCK(m, cudaStreamSynchronize(m->stream));
+    MCK(m, cudaMemcpy(m->params, host_in, mlp::NPARAM * 4, cudaMemcpyHostToDevice));
+    MCK(m, cudaMemset(m->adam_m, 0, mlp::NPARAM * 4));
+    MCK(m, cudaMemset(m->adam_v, 0, mlp::NPARAM * 4));
+    m->adam_step = 0;
+    return MPM_OK;
+}
+
+static int mlp_check_err(MpmMlp* m) {
+    uint32_t e = 0;
+    MCK(m, cudaMemcpy(&e, m->err, 4, cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(m->err, 0, 4);
+        return mlp_fail(m, MPM_ERR_DEVICE_STATUS, "tensor-core wait ran out (device status 0x%x)", e);
+    }
+    return MPM_OK;
+}
+
+extern "C" int mpm_mlp_forward(MpmMlp* m, const float* x_dev, uint32_t n, float* y_dev) {
+    if (!m || (n && (!x_dev || !y_dev))) return MPM_ERR_ARG;
+    if (n == 0) return MPM_OK;
+    cudaSetDevice(m->device);
+    int grid = (int)std::min<uint32_t>((n + 127u) / 128u, (uint32_t)m->n_sms * 4u);
+    MCK(m, launch_mlp_forward(m->params, x_dev, n, y_dev, m->err, grid, m->stream));
+    MCK(m, cudaStreamSynchronize(m->stream));
+    return mlp_check_err(m);
+}
+
+extern "C" int mpm_mlp_gradient(MpmMlp* m, const float* x_dev, const float* t_dev, uint32_t n, float unc_weight,
+                                float* grad_host, float* loss_host) {
+    if (!m || n == 0 || !x_dev || !t_dev) return MPM_ERR_ARG;
+    cudaSetDevice(m->device);
+    MCK(m, cudaMemsetAsync(m->grad, 0, mlp::NPARAM * 4, m->stream));
+    MCK(m, cudaMemsetAsync(m->loss, 0, 8, m->stream));
+    int grid = (int)std::min<uint32_t>((n + 127u) / 128u, (uint32_t)m->n_sms);
+    MCK(m, launch_mlp_train(m->params, x_dev, t_dev, nullptr, n, 1.0f / (float)n, unc_weight, m->grad, m->loss,
+                            m->err, grid, m->stream));
+    MCK(m, cudaStreamSynchronize(m->stream));
+    int r = mlp_check_err(m);
+    if (r) return r;
+    if (grad_host) MCK(m, cudaMemcpy(grad_host, m->grad, mlp::NPARAM * 4, cudaMemcpyDeviceToHost));
+    if (loss_host) MCK(m, cudaMemcpy(loss_host, m->loss, 4, cudaMemcpyDeviceToHost));
+    return MPM_OK;
+}
+
+extern "C" int mpm_mlp_train(MpmMlp* m, const float* x_dev, const float* t_dev, uint32_t n,
+                             const MpmMlpTrainConfig* cfg, float* loss_per_epoch) {
+    if (!m || !cfg || n == 0 || !x_dev || !t_dev) return MPM_ERR_ARG;
+    if (cfg->batch == 0 || cfg->epochs == 0) return mlp_fail(m, MPM_ERR_ARG, "batch and epochs must be > 0");
+    cudaSetDevice(m->device);
+    if (m->idx_cap < n) {
+        if (m->idx) cudaFree(m->idx);
+        m->idx = nullptr;
+        MCK(m, cudaMalloc(&m->idx, (size_t)n * 4));
+        m->idx_cap = n;
+    }
+    std::vector<uint32_t> perm(n);
+    uint64_t st = 0x747261696eull ^ cfg->seed;
+    const uint32_t n_batches = (n + cfg->batch - 1) / cfg->batch;
+    const uint32_t total = n_batches * cfg->epochs;
+    uint32_t step = 0;
+    for (uint32_t ep = 0; ep < cfg->epochs; ep++) {
+        for (uint32_t i = 0; i < n; i++) perm[i] = i;
+        for (uint32_t i = n - 1; i > 0; i--) {
+            uint32_t j = (uint32_t)(splitmix(st) % (uint64_t)(i + 1));
+            std::swap(perm[i], perm[j]);
+        }
+        MCK(m, cudaMemcpyAsync(m->idx, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+        MCK(m, cudaMemsetAsync(m->loss, 0, 8, m->stream));
+        for (uint32_t b = 0; b < n_batches; b++) {
+            uint32_t b0 = b * cfg->batch, nb = std::min(cfg->batch, n - b0);
+            MCK(m, cudaMemsetAsync(m->grad, 0, mlp::NPARAM * 4, m->stream));
+            int grid = (int)std::min<uint32_t>((nb + 127u) / 128u, (uint32_t)m->n_sms);
+            MCK(m, launch_mlp_train(m->params, x_dev, t_dev, m->idx + b0, nb, 1.0f / (float)nb, cfg->unc_weight,
+                                    m->grad, m->loss, m->err, grid, m->stream));
+            // cosine decay from lr to lr_final over all steps
+            float f = 0.5f * (1.0f + std::cos(3.14159265f * (float)step / (float)std::max(1u, total - 1u)));
+            float lr = cfg->lr_final + (cfg->lr - cfg->lr_final) * f;
+            m->adam_step++;
+            MCK(m, launch_adam(m->params, m->adam_m, m->adam_v, m->grad, mlp::NPARAM, lr, m->adam_step, m->stream));
+            step++;
+        }
+        float lsum = 0.f;
+        MCK(m, cudaMemcpyAsync(&lsum, m->loss, 4, cudaMemcpyDeviceToHost, m->stream));
+        MCK(m, cudaStreamSynchronize(m->stream));
+        int r = mlp_check_err(m);
+        if (r) return r;
+        if (loss_per_epoch) loss_per_epoch[ep] = lsum / (float)n_batches;
+    }
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_plasticity(MpmHandle* h, int mode, MpmMlp* net, float unc_threshold, float det_threshold,
+                                  float audit_fraction) {
+    if (!h) return MPM_ERR_ARG;
+    if (mode < MPM_PLASTICITY_INLINE || mode > MPM_PLASTICITY_LEARNED) return fail(h, MPM_ERR_ARG, "bad plasticity mode %d", mode);
+    if (mode == MPM_PLASTICITY_LEARNED && !net) return fail(h, MPM_ERR_ARG, "learned plasticity needs a network");
+    if (net && net->device != h->device) return fail(h, MPM_ERR_ARG, "network lives on device %d, handle on %d", net->device, h->device);
+    if (!(audit_fraction >= 0.f && audit_fraction <= 1.f)) return fail(h, MPM_ERR_ARG, "audit fraction must be in [0, 1]");
+    cudaSetDevice(h->device);
+    if (mode != MPM_PLASTICITY_INLINE && !h->plast_list)
+        CK(h, cudaMalloc(&h->plast_list, (size_t)h->cfg.max_particles * 4));
+    h->plast_mode = mode;
+    h->mlp = net;
+    h->unc_threshold = unc_threshold;
+    h->det_threshold = det_threshold;
+    h->audit_threshold = (uint32_t)std::min(4294967295.0, (double)audit_fraction * 4294967296.0);
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_pair_buffer(MpmHandle* h, float* x_dev, float* t_dev, uint32_t capacity) {
+    if (!h) return MPM_ERR_ARG;
+    if (capacity && (!x_dev || !t_dev)) return fail(h, MPM_ERR_ARG, "null pair buffer");
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->pair_x = capacity ? x_dev : nullptr;
+    h->pair_t = capacity ? t_dev : nullptr;
+    h->pair_cap = capacity;
+    CK(h, cudaMemset(h->d_pair_count, 0, 4));
+    return MPM_OK;
+}
+
+extern "C" int mpm_get_plasticity_stats(MpmHandle* h, MpmPlasticityStats* out, int reset) {
+    if (!h || !out) return MPM_ERR_ARG;
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    PlastStats ps;
+    uint32_t pairs = 0;
+    CK(h, cudaMemcpy(&ps, h->d_stats, sizeof(ps), cudaMemcpyDeviceToHost));
+    CK(h, cudaMemcpy(&pairs, h->d_pair_count, 4, cudaMemcpyDeviceToHost));
+    out->candidates = ps.candidates;
+    out->learned = ps.learned;
+    out->fallback_domain = ps.fallback_domain;
+    out->fallback_uncertain = ps.fallback_uncertain;
+    out->fallback_det = ps.fallback_det;
+    out->audited = ps.audited;
+    float mx;
+    std::memcpy(&mx, &ps.audit_max_err_bits, 4);
+    out->audit_max_err = mx;
+    out->audit_mean_err = ps.audited ? (float)(ps.audit_err_sum / (double)ps.audited) : 0.f;
+    out->pairs_collected = std::min(pairs, h->pair_cap);
+    if (reset) CK(h, cudaMemset(h->d_stats, 0, sizeof(PlastStats)));
     return MPM_OK;
 }
 

@@ -49,6 +49,7 @@ constexpr uint32_t ST_TILE_OVERFLOW = 0x2u;
 constexpr uint32_t ST_BVH_STACK = 0x4u;
 constexpr uint32_t ST_SCENE_RANGE = 0x8u;
 constexpr uint32_t ST_MLP_FALLBACK = 0x10u;
+constexpr uint32_t ST_MLP_TIMEOUT = 0x20u;
 
 
 // Per-scene parameters: the uniform fields the step reads plus the
@@ -94,7 +95,9 @@ struct Counters {
     uint32_t n_st;       // occupied tiles of the current substep
     uint32_t n_binned;   // particles placed in tiles
     uint32_t status;     // sticky status bits
-    uint32_t pad;
+    uint32_t n_plast;    // deferred plasticity candidates of the current substep
+    uint32_t step;       // substeps run on this buffer (advanced at each substep's start)
+    uint32_t pad[3];
 };
 
 struct Ctx {
@@ -117,6 +120,8 @@ struct Ctx {
     int4* tiles_b;            // tiles read by this pass's G2P
     float4* iter_rec;         // PBMPM iteration records, IR_PLANES x n float4, sorted order
     int32_t* st_nbr;          // per compact tile, the compact index of its 27 neighbours (-1: none)
+    uint32_t* plast_list;     // deferred plasticity: particles the strain-bound check did not clear
+    uint32_t plast_defer;     // 0: exact return map inside integrate; 1: deferred to the plasticity pass
     const SceneDev* scenes;
     const uint32_t* scene_first;  // n_scenes + 1 particle offsets
     Counters* counters;
@@ -151,6 +156,7 @@ enum KernelId : uint32_t {
     K_G2P_PBMPM,
     K_GRID_DENSE,
     K_TILE_NBR,
+    K_PLASTICITY,
     K_COUNT
 };
 

@@ -14,6 +14,7 @@
 // written once with plain 16-byte stores.
 #include "mpm_engine.cuh"
 #include "mpm_math.cuh"
+#include "mpm_plast.cuh"
 
 namespace mpm {
 
@@ -235,25 +236,9 @@ __device__ __forceinline__ void pbmpm_constraints(const SceneDev& S, const float
     }
 }
 
-// applyPlasticity (plasticityOps.wgsl:7-48)
+// applyPlasticity (plasticityOps.wgsl:7-48), in mpm_plast.cuh
 __device__ __forceinline__ void plasticity(const SceneDev& S, float* Fe, float* Fp) {
-    float R[9], Rt[9], Sm[9];
-    polar3(Fe, R);
-    tr3(R, Rt);
-    mul3(Rt, Fe, Sm);
-    float sg0 = Sm[0], sg1 = Sm[4], sg2 = Sm[8];
-    if (S.smin <= sg0 && S.smin <= sg1 && S.smin <= sg2 && sg0 <= S.smax && sg1 <= S.smax && sg2 <= S.smax) return;
-    float c0 = fminf(fmaxf(sg0, S.smin), S.smax);
-    float c1 = fminf(fmaxf(sg1, S.smin), S.smax);
-    float c2 = fminf(fmaxf(sg2, S.smin), S.smax);
-    float Dg[9] = {c0, 0.f, 0.f, 0.f, c1, 0.f, 0.f, 0.f, c2};
-    float Fn[9], Fni[9], F[9];
-    mul3(R, Dg, Fn);
-    inv3(Fn, Fni);
-    mul3(Fe, Fp, F);
-    mul3(Fni, F, Fp);
-#pragma unroll
-    for (int i = 0; i < 9; i++) Fe[i] = Fn[i];
+    plasticity_exact(S.smin, S.smax, Fe, Fp);
 }
 
 // ------------------------------------------------------------------
@@ -484,15 +469,32 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
     }
 }
 
-// integrateParticles (integrateParticles.wgsl:14-72)
-__device__ __forceinline__ void integrate(const SceneDev& S, PState& p, Counters* ctr) {
+// Appends particle pid to the deferred plasticity list (warp-aggregated).
+__device__ __forceinline__ void defer_plasticity(const Ctx& c, uint32_t pid) {
+    unsigned m = __activemask();
+    int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&c.counters->n_plast, (uint32_t)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    c.plast_list[base + (uint32_t)__popc(m & lanemask_lt())] = pid;
+}
+
+// integrateParticles (integrateParticles.wgsl:14-72).  With deferred
+// plasticity the record keeps the trial Fe; particles the strain-bound check
+// does not clear are listed for the plasticity pass (exact or learned).
+__device__ __forceinline__ void integrate(const Ctx& c, const SceneDev& S, PState& p, uint32_t pid) {
+    Counters* ctr = c.counters;
 #pragma unroll
     for (int k = 0; k < 3; k++) p.pos[k] = fa(p.pos[k], p.dxp[k]);
     float IpD[9];
 #pragma unroll
     for (int i = 0; i < 9; i++) IpD[i] = fa((i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f, p.D[i]);
     mul3(IpD, p.Fe, p.Fe);
-    plasticity(S, p.Fe, p.Fp);
+    if (c.plast_defer) {
+        if (!cert_elastic(S.smin, S.smax, p.Fe)) defer_plasticity(c, pid);
+    } else {
+        plasticity(S, p.Fe, p.Fp);
+    }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         if (p.pos[a] < S.gmin[a]) { p.dxp[a] = fm(p.dxp[a], S.rest); p.pos[a] = S.gmin[a]; p.vel[a] = fm(p.vel[a], S.rest); }
@@ -506,6 +508,10 @@ __device__ __forceinline__ void integrate(const SceneDev& S, PState& p, Counters
 // ------------------------------------------------------------------
 __global__ void k_clear_table(Ctx c) {
     uint32_t n = c.counters->n_st;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.counters->n_plast = 0u;
+        c.counters->step += 1u;
+    }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t s = c.st_slot[i];
         c.keys[s] = KEY_EMPTY;
@@ -1258,7 +1264,7 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
             float nv[3], G[9];
             g2p_gather<E, PB>(T, vel, sc, nv, G);
             g2p_finish<PB>(S, nv, G, p.vel, p.dxp, p.D);
-            integrate(S, p, c.counters);
+            integrate(c, S, p, pid);
             store_particle(rec, p);
         }
         __syncthreads();
