@@ -335,6 +335,169 @@ def gpu_run(args, rank, world, local):
     return out
 
 
+# ----------------------------------------------------------------------
+# extra legs at N = 1: learned plasticity (config 4) and batched scenes (config 3)
+# ----------------------------------------------------------------------
+def _events(torch, stream):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _pipeline(pkg, spec, tile_edge, stream, local, max_tiles=0):
+    buf = pkg.GpuMpmBufferManager(n_particles=spec.particles.shape[0], device=local, tile_edge=tile_edge,
+                                  stream=stream.cuda_stream, max_tiles=max_tiles)
+    buf.write_particles(spec.particles)
+    col = None
+    if spec.mesh is not None:
+        col = pkg.GpuColliderBufferManager(vertices=spec.mesh[0], indices=spec.mesh[1])
+    pipe = pkg.GpuMpmPipelineManager(mpm_manager=buf, uniforms_manager=spec.uniforms, collider_manager=col,
+                                     params=make_params(pkg, spec.params))
+    return buf, pipe
+
+
+def _agg(rec):
+    import numpy as np
+    m = rec["mass"].astype(np.float64)
+    com = (rec["pos"].astype(np.float64) * m[:, None]).sum(0) / m.sum()
+    mom = (rec["vel"].astype(np.float64) * m[:, None]).sum(0)
+    F = rec["Fp"][:, :, :3].astype(np.float64)
+    jp = float(np.linalg.det(F).mean())
+    return com, mom, jp
+
+
+def _agg_rel_err(a, b):
+    import numpy as np
+    return {"centre_of_mass": float(np.abs(a[0] - b[0]).max()),
+            "momentum": float(np.abs(a[1] - b[1]).max() / max(np.abs(b[1]).max(), 1e-30)),
+            "mean_jp": float(abs(a[2] - b[2]) / abs(b[2]))}
+
+
+def _timed_run(pkg, torch, spec, mode, net, tile_edge, stream, local, warmup, steps):
+    """(particle-substeps/s, final records, plasticity stats) of `steps`
+    graph-replayed PBMPM substeps from the scene's initial state."""
+    # fixed tile storage: the pre-compacted snow spreads while it relaxes
+    buf, pipe = _pipeline(pkg, spec, tile_edge, stream, local, max_tiles=6 * 4732)
+    ctl = pkg.learned.PlasticityController(buf)
+    ctl.set_mode(mode, net, unc_threshold=0.2, det_threshold=1e-3, audit_fraction=0.01)
+    method = pkg.GpuSimulationMethodType.Pbmpm
+    for _ in range(warmup):
+        pipe.step(method, 1)
+    buf.sync()
+    ctl.stats(reset=True)
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    for _ in range(steps):
+        pipe.step(method, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    rate = spec.particles.shape[0] * steps / (e0.elapsed_time(e1) * 1e-3)
+    st = ctl.stats()
+    buf.sync()
+    rec = buf.read_particles()
+    buf.close()
+    return rate, rec, st
+
+
+def surrogate_leg(pkg, args, local, stream):
+    import numpy as np
+    import torch
+
+    L = pkg._lib
+    rng = np.random.default_rng(41)
+    t0 = time.perf_counter()
+    xs, ts, mats = [], [], []
+    for r in range(4):
+        E, tc = float(rng.uniform(5e4, 3e5)), float(rng.uniform(1.5e-2, 3.5e-2))
+        spec = pkg.scenes.c4_prestrained(counts=(128, 32, 128), seed=50 + r, youngs_modulus=E, theta_c=tc)
+        buf, pipe = _pipeline(pkg, spec, args.tile_edge, stream, local, max_tiles=6 * 1183)
+        ctl = pkg.learned.PlasticityController(buf)
+        ctl.set_mode(L.PLASTICITY_COLLECT, audit_fraction=0.1)
+        x, t = ctl.collect_into(2_500_000, device=local)
+        for k in range(80):
+            pipe.step(pkg.GpuSimulationMethodType.Pbmpm, 1)
+        n = ctl.stats()["pairs_collected"]
+        xs.append(x[:n].clone())
+        ts.append(t[:n].clone())
+        mats.append({"E": round(E, 1), "theta_c": round(tc, 5), "pairs": int(n)})
+        buf.close()
+        del x, t
+    x, t = torch.cat(xs), torch.cat(ts)
+    torch.cuda.synchronize()
+    collect_s = time.perf_counter() - t0
+    net = pkg.learned.PlasticityNet(device=local, seed=7)
+    net.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    hist = net.train(x, t, epochs=8, batch=8192, lr=3e-3, lr_final=3e-5, unc_weight=0.1, seed=3)
+    train_s = time.perf_counter() - t0
+    # network throughput on 4,194,304 rows (tensor-core forward alone)
+    rows = 4194304
+    xr = x[torch.randint(0, x.shape[0], (rows,), device=x.device)].contiguous()
+    net.forward(xr)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    for _ in range(5):
+        net.forward(xr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / 5
+    flops = 2.0 * (12 * 64 + 64 * 64 * 2 + 64 * 11) * rows
+    del xr, x, t, xs, ts
+    out = {"train": {"pairs": int(sum(m["pairs"] for m in mats)), "rollouts": mats, "collect_s": round(collect_s, 2),
+                     "train_s": round(train_s, 2), "epochs": 8, "batch": 8192,
+                     "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1])},
+           "mlp_forward": {"rows": rows, "ms": round(fwd_ms, 4), "tflops": round(flops / (fwd_ms * 1e-3) / 1e12, 2)}}
+    steps, warm = max(10, min(args.steps, 40)), 3
+    for name, spec in (("c2_large_pbmpm", build_scene(pkg, counts=args.counts)),
+                       ("c4_prestrained", pkg.scenes.c4_prestrained(counts=args.counts))):
+        r_plain, rec_p, _ = _timed_run(pkg, torch, spec, L.PLASTICITY_INLINE, None, args.tile_edge, stream, local,
+                                       warm, steps)
+        r_learn, rec_l, st = _timed_run(pkg, torch, spec, L.PLASTICITY_LEARNED, net, args.tile_edge, stream, local,
+                                        warm, steps)
+        st = {k: (int(v) if isinstance(v, int) else float(v)) for k, v in st.items()}
+        out[name] = {"substeps": warm + steps, "plain": r_plain, "learned": r_learn, "vs_plain": r_learn / r_plain,
+                     "agg_rel_err_vs_plain": _agg_rel_err(_agg(rec_l), _agg(rec_p)), "stats": st}
+        del rec_p, rec_l
+    net.close()
+    return out
+
+
+def batched_leg(pkg, args, local, stream):
+    import torch
+
+    specs = pkg.scenes.c3_batched()
+    method = pkg.GpuSimulationMethodType.ExplicitMpm
+    n_total = int(sum(s.particles.shape[0] for s in specs))
+    best, times = pkg.batching.autotune_tile_edge(specs, method, steps=3, device=local)
+    b = pkg.GpuMpmBatch(specs, device=local, tile_edge=best, stream=stream.cuda_stream)
+    steps = max(10, min(args.steps, 30))
+    ms = pkg.batching.time_batch(b, method, steps, warmup=3)
+    b.close()
+    # the plain per-scene loop: one handle per scene, launched one after another
+    handles = []
+    for spec in specs:
+        buf, pipe = _pipeline(pkg, spec, best, stream, local)
+        handles.append((buf, pipe))
+    for buf, pipe in handles:
+        pipe.step(method, 2)
+    torch.cuda.synchronize()
+    loop_steps = 5
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    for _ in range(loop_steps):
+        for buf, pipe in handles:
+            pipe.step(method, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    loop_ms = e0.elapsed_time(e1) / loop_steps
+    for buf, _ in handles:
+        buf.close()
+    return {"workload": f"c3_batched: {len(specs)} scenes, {n_total:,} particles, explicit, dx 1/64 or 1/128",
+            "tile_edge_autotuned": best, "autotune_ms_per_substep": {str(k): round(v, 4) for k, v in times.items()},
+            "batched_ms_per_substep": round(ms, 4), "batched_value": n_total / (ms * 1e-3),
+            "per_scene_loop_ms_per_substep": round(loop_ms, 4), "per_scene_loop_value": n_total / (loop_ms * 1e-3),
+            "batched_vs_loop": loop_ms / ms, "unit": "particle-substeps/s"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,6 +506,8 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--tile-edge", type=int, default=16)
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the learned-plasticity and batched-scene legs (they run at N = 1 only)")
     ap.add_argument("--counts", default="256,64,256",
                     help="slab lattice size x,y,z (default: the full 4,194,304-particle workload; smaller "
                          "lattices give the small cases used for profiling)")
@@ -371,6 +536,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     out = gpu_run(args, rank, world, local)
+    if world == 1 and not args.no_extra:
+        import torch
+        stream = torch.cuda.current_stream()
+        out["surrogate"] = surrogate_leg(importlib.import_module(PKG), args, local, stream)
+        out["batched"] = batched_leg(importlib.import_module(PKG), args, local, stream)
     if rank == 0:
         rate, cores, sample, _ = cpu_reference(args.cpu_steps, 0)
         out["cpu_baseline"] = {"value": rate, "unit": "particle-substeps/s", "cores": cores, "kind": "port",

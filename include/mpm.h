@@ -182,9 +182,10 @@ int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* ident_mismatch
  *           Fe^T Fe inside the elastic band, so the exact map would return
  *           its input unchanged) and lists the rest; a separate pass runs
  *           the exact map on them.  Results equal INLINE bit for bit;
- *   COLLECT as EXACT, and each listed particle inside the trained domain
- *           also writes a training pair (12 inputs, 10 targets) to the
- *           buffer given by mpm_set_pair_buffer;
+ *   COLLECT as EXACT, and a sampled fraction (audit_fraction, drawn per
+ *           particle and substep) of the listed particles inside the trained
+ *           domain also writes a training pair (12 inputs, 10 targets) to
+ *           the buffer given by mpm_set_pair_buffer;
  *   LEARNED as EXACT, but the pass runs the network (BF16 tensor cores,
  *           FP32 accumulation) and takes its answer unless the particle is
  *           outside the trained domain, the uncertainty output exceeds
@@ -220,9 +221,9 @@ typedef struct MpmMlpTrainConfig {
 } MpmMlpTrainConfig;
 
 typedef struct MpmPlasticityStats {
-    uint64_t candidates;          /* particles the strain-bound check did not clear */
+    uint64_t candidates;          /* particles the strain-bound check did not clear (all deferred modes) */
     uint64_t learned;             /* took the network's answer */
-    uint64_t fallback_domain;     /* exact: outside the trained domain */
+    uint64_t fallback_domain;     /* outside the trained domain (exact map; in COLLECT mode: no pair) */
     uint64_t fallback_uncertain;  /* exact: uncertainty above threshold */
     uint64_t fallback_det;        /* exact: determinant check failed */
     uint64_t audited;             /* exact, with the network's error recorded */
@@ -237,6 +238,9 @@ int mpm_mlp_init_params(uint32_t seed, float* out);
 int mpm_mlp_create(int device, uint32_t seed, MpmMlp** out);
 int mpm_mlp_destroy(MpmMlp* m);
 const char* mpm_mlp_last_error(const MpmMlp* m);
+/* Orders the network's work on the caller's cudaStream_t (NULL: a private
+ * stream, the default).  Calls still return after their work completes. */
+int mpm_mlp_set_stream(MpmMlp* m, void* stream);
 int mpm_mlp_get_params(MpmMlp* m, float* host_out);
 int mpm_mlp_set_params(MpmMlp* m, const float* host_in);
 /* Network outputs for n inputs (device arrays [n][12] -> [n][11]); synchronous. */

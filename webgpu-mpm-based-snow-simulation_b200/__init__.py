@@ -6,15 +6,15 @@ records come out.  Compute runs in libmpm.so (include/mpm.h); this package is
 the host-side mirror of the reference's TypeScript managers plus scene
 generators.
 """
-from . import _lib, layout, learned, scenes
+from . import _lib, batching, layout, learned, scenes
 from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams, default_params, load
 from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
-from .pipeline import (GpuColliderBufferManager, GpuMpmBufferManager, GpuMpmPipelineManager,
+from .pipeline import (GpuColliderBufferManager, GpuMpmBatch, GpuMpmBufferManager, GpuMpmPipelineManager,
                        GpuSimulationMethodType, build_bvh, kernel_names)
 
 __all__ = [
     "METHOD_EXPLICIT", "METHOD_PBMPM", "MpmConfig", "MpmError", "MpmParams", "default_params", "load",
     "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
-    "GpuMpmBufferManager", "GpuMpmPipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
-    "layout", "scenes", "learned",
+    "GpuMpmBufferManager", "GpuMpmBatch", "GpuMpmPipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
+    "layout", "scenes", "learned", "batching",
 ]

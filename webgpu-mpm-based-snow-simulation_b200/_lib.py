@@ -131,6 +131,7 @@ SIGNATURES = {
     "mpm_mlp_create": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_void_p)]),
     "mpm_mlp_destroy": (C.c_int, [C.c_void_p]),
     "mpm_mlp_last_error": (C.c_char_p, [C.c_void_p]),
+    "mpm_mlp_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mpm_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mpm_mlp_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mpm_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),

@@ -53,6 +53,7 @@ struct MpmMlp {
     int device = 0;
     int n_sms = 0;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;
     float* params = nullptr;   // NPARAM FP32 masters
     float* adam_m = nullptr;
     float* adam_v = nullptr;
@@ -1086,12 +1087,27 @@ extern "C" int mpm_mlp_destroy(MpmMlp* m) {
     void* bufs[] = {m->params, m->adam_m, m->adam_v, m->grad, m->loss, m->err, m->idx};
     for (void* b : bufs)
         if (b) cudaFree(b);
-    if (m->stream) cudaStreamDestroy(m->stream);
+    if (m->stream && m->own_stream) cudaStreamDestroy(m->stream);
     delete m;
     return MPM_OK;
 }
 
 extern "C" const char* mpm_mlp_last_error(const MpmMlp* m) { return m ? m->msg.c_str() : "null network"; }
+
+extern "C" int mpm_mlp_set_stream(MpmMlp* m, void* stream) {
+    if (!m) return MPM_ERR_ARG;
+    cudaSetDevice(m->device);
+    MCK(m, cudaStreamSynchronize(m->stream));
+    if (m->own_stream) cudaStreamDestroy(m->stream);
+    if (stream) {
+        m->stream = (cudaStream_t)stream;
+        m->own_stream = false;
+    } else {
+        MCK(m, cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+        m->own_stream = true;
+    }
+    return MPM_OK;
+}
 
 extern "C" int mpm_mlp_get_params(MpmMlp* m, float* host_out) {
     if (!m || !host_out) return MPM_ERR_ARG;

@@ -200,6 +200,7 @@ __device__ __forceinline__ void mlp_targets(const float* Fe, const float* Fp, co
 template <int MODE>
 __global__ void __launch_bounds__(128) k_plasticity_exact(Ctx c, PlastCtx pc) {
     const uint32_t count = c.counters->n_plast;
+    const uint32_t step = c.counters->step;
     {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
             uint32_t pid = c.plast_list[i];
@@ -208,10 +209,12 @@ __global__ void __launch_bounds__(128) k_plasticity_exact(Ctx c, PlastCtx pc) {
             float Fe[9], Fp[9], x[12];
             load_fe_fp(rec, Fe, Fp);
             bool dom = mlp_features(Fe, Fp, S.dt, 1.0f - S.smin, x);
+            warp_count(&pc.stats->candidates, true);
+            warp_count(&pc.stats->fallback_domain, !dom);
             float Fe2[9], Fp2[9];
             for (int k = 0; k < 9; k++) { Fe2[k] = Fe[k]; Fp2[k] = Fp[k]; }
             plasticity_exact(S.smin, S.smax, Fe2, Fp2);
-            if (MODE == PLAST_COLLECT && dom && pc.pair_x) {
+            if (MODE == PLAST_COLLECT && dom && pc.pair_x && hash3(pid, step, 0xc011u) < pc.audit_threshold) {
                 uint32_t slot = atomicAdd(pc.pair_count, 1u);
                 if (slot < pc.pair_cap) {
                     float t[10];

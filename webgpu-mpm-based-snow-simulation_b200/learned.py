@@ -58,6 +58,10 @@ class PlasticityNet:
         except Exception:
             pass
 
+    def set_stream(self, stream: int | None) -> None:
+        """Orders the network's kernels on a CUDA stream handle (None: private)."""
+        self._check(self._lib.mpm_mlp_set_stream(self.handle, C.c_void_p(stream) if stream else None))
+
     @staticmethod
     def init_params(seed: int) -> np.ndarray:
         out = np.zeros(PARAMS, np.float32)
@@ -115,6 +119,8 @@ class PlasticityController:
 
     def set_mode(self, mode: int, net: PlasticityNet | None = None, *, unc_threshold: float = 0.05,
                  det_threshold: float = 1e-3, audit_fraction: float = 0.01) -> None:
+        """audit_fraction: LEARNED, the audited share of the network's answers;
+        COLLECT, the sampled share of listed particles that write a pair."""
         self.net = net
         check(self._lib.mpm_set_plasticity(self.mpm.handle, mode, net.handle if net else None, unc_threshold,
                                            det_threshold, audit_fraction), self.mpm.handle)

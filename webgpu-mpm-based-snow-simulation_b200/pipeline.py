@@ -208,6 +208,65 @@ class GpuMpmPipelineManager:
         check(self._lib.mpm_step(self.mpm.handle, int(method), n_substeps), self.mpm.handle)
 
 
+class GpuMpmBatch:
+    """Many independent scenes advanced by the same launches: one handle, one
+    scene table, particles concatenated in scene order.  Each scene keeps its
+    own uniform block, extension parameters, grid and collider (a
+    GpuMpmPipelineManager per scene sets them up); a substep bins every
+    scene's particles into one tile table keyed by (scene, tile) and runs each
+    kernel once over all tiles, captured in one CUDA graph.  The reference
+    runs one scene per device; this is the batched form of its step."""
+
+    def __init__(self, specs, *, device: int = 0, tile_edge: int = 16, stream: int | None = None):
+        lib = load()
+        self.specs = list(specs)
+        counts = [int(s.particles.shape[0]) for s in self.specs]
+        n = int(sum(counts))
+        self.mpm = GpuMpmBufferManager(n_particles=n, device=device, max_scenes=len(self.specs),
+                                       tile_edge=tile_edge, stream=stream)
+        h = self.mpm.handle
+        check(lib.mpm_set_scene_count(h, len(self.specs)), h)
+        self.ranges = []
+        first = 0
+        for i, c in enumerate(counts):
+            check(lib.mpm_set_scene_range(h, i, first, c), h)
+            self.ranges.append((first, c))
+            first += c
+        self.pipes = []
+        for i, spec in enumerate(self.specs):
+            col = None
+            if spec.mesh is not None:
+                col = GpuColliderBufferManager(vertices=spec.mesh[0], indices=spec.mesh[1])
+            prm = _lib.default_params()
+            for k, v in spec.params.items():
+                if k == "gravity":
+                    prm.gravity[:] = [float(x) for x in v]
+                else:
+                    setattr(prm, k, v)
+            self.pipes.append(GpuMpmPipelineManager(mpm_manager=self.mpm, uniforms_manager=spec.uniforms,
+                                                    collider_manager=col, params=prm, scene=i))
+        self.mpm.write_particles(np.concatenate([s.particles for s in self.specs]))
+        self._lib = lib
+
+    @property
+    def n_particles(self) -> int:
+        return self.mpm.n_particles
+
+    def step(self, method: GpuSimulationMethodType, n_substeps: int = 1) -> None:
+        for p in self.pipes:
+            p.uniforms.write_use_pbmpm(method == GpuSimulationMethodType.Pbmpm)
+            p.push_uniforms()
+        check(self._lib.mpm_step(self.mpm.handle, int(method), n_substeps), self.mpm.handle)
+
+    def scene_particles(self, i: int, records: np.ndarray | None = None) -> np.ndarray:
+        rec = self.mpm.read_particles() if records is None else records
+        a, c = self.ranges[i]
+        return rec[a:a + c]
+
+    def close(self) -> None:
+        self.mpm.close()
+
+
 def kernel_names() -> list[str]:
     lib = load()
     return [lib.mpm_kernel_name(i).decode() for i in range(lib.mpm_kernel_count())]

@@ -197,11 +197,17 @@ def config_params(dx, **over):
     return p
 
 
-def _particles_from(pos, mass, vel):
+def _particles_from(pos, mass, vel, pbmpm_dt=None):
+    """Particle records at rest shape (F_e = F_p = I).  PBMPM's first transfer
+    carries momentum from the displacement field (pbmpm.wgsl:67), not from
+    the velocity, so a PBMPM scene passes its timestep and the initial
+    velocity is also written as the displacement v * dt."""
     p = new_particles(pos.shape[0])
     p["pos"] = pos
     p["mass"] = mass
     p["vel"] = np.asarray(vel, np.float32)
+    if pbmpm_dt is not None:
+        p["dxp"] = p["vel"] * np.float32(pbmpm_dt)
     return p
 
 
@@ -246,7 +252,7 @@ def c1_pbmpm_spheres(n_per_sphere=131072, seed=1, n_iter=6, parity=False, with_c
     u = make_uniforms([0, 0, 0], [1, 1, 1], res, 2e-4, 2.0 ** 39, mesh=mesh)
     params = reference_params(n_iter=n_iter, force_divisor=float(n_iter)) if parity else \
         config_params(1 / 128, n_iter=n_iter, force_divisor=float(n_iter))
-    return SceneSpec("c1_pbmpm_spheres", u, params, _particles_from(pos, mass, vel), 1, 100, mesh, res,
+    return SceneSpec("c1_pbmpm_spheres", u, params, _particles_from(pos, mass, vel, pbmpm_dt=2e-4), 1, 100, mesh, res,
                      {"spacing": spacing})
 
 
@@ -264,6 +270,27 @@ def c2_large_pbmpm(counts=(256, 64, 256), seed=2, n_iter=6, terrain_n=256):
     params = config_params(1 / 512, n_iter=n_iter, force_divisor=float(n_iter))
     return SceneSpec("c2_large_pbmpm", u, params, _particles_from(pos, mass, (0.0, 0.0, 0.0)), 1, 200, mesh, res,
                      {"spacing": spacing, "ppc": (1 / 512) ** 3 / spacing ** 3})
+
+
+def c4_prestrained(counts=(256, 64, 256), seed=4, n_iter=6, youngs_modulus=1.4e5, theta_c=2.5e-2, prestrain=0.01):
+    """The large PBMPM scene with its return map active: c2_large_pbmpm (same
+    slab, grid, dt, terrain) with pre-compacted snow, each particle's F_e
+    drawn as I + N(0, prestrain^2) per entry, so most particles start beyond
+    the elastic band and, once clamped, sit on the yield surface.  (With the
+    reference's transfers the deformation rate is measured in cell units, so
+    at dx = 1/512 the deformation of c2_large_pbmpm itself stays inside the
+    elastic band and its return map never acts.)  Used to generate the
+    learned plasticity's training pairs, with randomised E and theta_c, and
+    to time the learned form where it does work."""
+    spec = c2_large_pbmpm(counts=counts, seed=seed, n_iter=n_iter)
+    rng = np.random.default_rng(seed + 1000)
+    n = spec.particles.shape[0]
+    Fe = np.eye(3, dtype=np.float32)[None] + rng.normal(0.0, prestrain, (n, 3, 3)).astype(np.float32)
+    spec.particles["Fe"][:, :, :3] = Fe
+    spec.params.update(youngs_modulus=youngs_modulus, theta_c=theta_c)
+    spec.name = "c4_prestrained"
+    spec.notes.update({"E": youngs_modulus, "theta_c": theta_c, "prestrain": prestrain})
+    return spec
 
 
 def c3_batched(n_scenes=256, seed=3, lo_count=2000, hi_count=200000):
