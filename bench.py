@@ -355,20 +355,25 @@ def _pipeline(pkg, spec, tile_edge, stream, local, max_tiles=0):
 
 
 def _agg(rec):
+    """Centre of mass, total momentum, total absolute momentum, mean J_p."""
     import numpy as np
     m = rec["mass"].astype(np.float64)
+    v = rec["vel"].astype(np.float64)
     com = (rec["pos"].astype(np.float64) * m[:, None]).sum(0) / m.sum()
-    mom = (rec["vel"].astype(np.float64) * m[:, None]).sum(0)
+    mom = (v * m[:, None]).sum(0)
+    abs_mom = float((np.linalg.norm(v, axis=1) * m).sum())
     F = rec["Fp"][:, :, :3].astype(np.float64)
     jp = float(np.linalg.det(F).mean())
-    return com, mom, jp
+    return com, mom, abs_mom, jp
 
 
 def _agg_rel_err(a, b):
+    """Relative deviation of a from b: centre of mass over the unit domain,
+    momentum over the total absolute momentum, mean J_p over itself."""
     import numpy as np
     return {"centre_of_mass": float(np.abs(a[0] - b[0]).max()),
-            "momentum": float(np.abs(a[1] - b[1]).max() / max(np.abs(b[1]).max(), 1e-30)),
-            "mean_jp": float(abs(a[2] - b[2]) / abs(b[2]))}
+            "momentum": float(np.abs(a[1] - b[1]).max() / max(b[2], 1e-30)),
+            "mean_jp": float(abs(a[3] - b[3]) / abs(b[3]))}
 
 
 def _timed_run(pkg, torch, spec, mode, net, tile_edge, stream, local, warmup, steps):
@@ -377,7 +382,7 @@ def _timed_run(pkg, torch, spec, mode, net, tile_edge, stream, local, warmup, st
     # fixed tile storage: the pre-compacted snow spreads while it relaxes
     buf, pipe = _pipeline(pkg, spec, tile_edge, stream, local, max_tiles=6 * 4732)
     ctl = pkg.learned.PlasticityController(buf)
-    ctl.set_mode(mode, net, unc_threshold=0.2, det_threshold=1e-3, audit_fraction=0.01)
+    ctl.set_mode(mode, net, unc_threshold=0.05, det_threshold=1e-3, audit_fraction=0.01)
     method = pkg.GpuSimulationMethodType.Pbmpm
     for _ in range(warmup):
         pipe.step(method, 1)
@@ -426,7 +431,8 @@ def surrogate_leg(pkg, args, local, stream):
     net = pkg.learned.PlasticityNet(device=local, seed=7)
     net.set_stream(stream.cuda_stream)
     t0 = time.perf_counter()
-    hist = net.train(x, t, epochs=8, batch=8192, lr=3e-3, lr_final=3e-5, unc_weight=0.1, seed=3)
+    epochs = 24
+    hist = net.train(x, t, epochs=epochs, batch=8192, lr=3e-3, lr_final=2e-5, unc_weight=0.1, seed=3)
     train_s = time.perf_counter() - t0
     # network throughput on 4,194,304 rows (tensor-core forward alone)
     rows = 4194304
@@ -443,7 +449,7 @@ def surrogate_leg(pkg, args, local, stream):
     flops = 2.0 * (12 * 64 + 64 * 64 * 2 + 64 * 11) * rows
     del xr, x, t, xs, ts
     out = {"train": {"pairs": int(sum(m["pairs"] for m in mats)), "rollouts": mats, "collect_s": round(collect_s, 2),
-                     "train_s": round(train_s, 2), "epochs": 8, "batch": 8192,
+                     "train_s": round(train_s, 2), "epochs": epochs, "batch": 8192,
                      "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1])},
            "mlp_forward": {"rows": rows, "ms": round(fwd_ms, 4), "tflops": round(flops / (fwd_ms * 1e-3) / 1e12, 2)}}
     steps, warm = max(10, min(args.steps, 40)), 3

@@ -59,7 +59,7 @@ typedef struct MpmConfig {
     uint32_t max_scenes;     /* 1 for a single scene */
     uint32_t max_tiles;      /* occupied grid tiles per substep (0: derived) */
     uint32_t hash_capacity;  /* tile hash slots, rounded up to a power of two (0: derived) */
-    uint32_t tile_edge;      /* grid tile edge in cells: 8, 12 or 16 (0: 16) */
+    uint32_t tile_edge;      /* grid tile edge in cells: 8, 12, 14 or 16 (0: 16) */
     int32_t device;          /* CUDA device ordinal */
     void* stream;            /* cudaStream_t to order work on, or NULL for a private stream */
 } MpmConfig;

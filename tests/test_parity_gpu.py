@@ -98,15 +98,19 @@ def test_small_and_ragged_counts(gpu, oracle_mod, n):
     g.close()
 
 
-def test_tile_edges_agree(gpu, oracle_mod):
-    spec = _scene(gpu, kind="pbmpm", with_collider=True)
+@pytest.mark.parametrize("kind", ["pbmpm", "explicit"])
+def test_tile_edges_agree(gpu, oracle_mod, kind):
+    spec = _scene(gpu, kind=kind, with_collider=True)
     outs = []
-    for e in (8, 16):
+    for e in (8, 12, 14, 16):
         g = GpuScene(gpu, spec, tile_edge=e)
         assert g.step(3) == 0
         outs.append(g.particles())
         g.close()
-    compare_states(outs[0], outs[1])
+    for o in outs[1:]:
+        compare_states(o, outs[0])
+    _, want = run_oracle(oracle_mod, spec, n_steps=3)
+    compare_states(outs[0], want)
 
 
 def test_graph_and_eager_agree(gpu):

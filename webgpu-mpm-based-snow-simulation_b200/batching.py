@@ -15,7 +15,7 @@ import heapq
 
 import numpy as np
 
-TILE_EDGES = (8, 12, 16)
+TILE_EDGES = (8, 12, 14, 16)
 
 
 def shard_scenes(counts, world: int) -> list[list[int]]:

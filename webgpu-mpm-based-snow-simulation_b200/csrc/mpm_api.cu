@@ -98,7 +98,8 @@ struct MpmHandle {
     uint32_t* st_count = nullptr;
     uint32_t* chunk_nst = nullptr;
     uint32_t* chunk_np = nullptr;
-    int4* tiles[2] = {nullptr, nullptr};
+    int4* tiles[3] = {nullptr, nullptr, nullptr};   // first transfer, then the PBMPM iterations' ping-pong
+    float* tile_rm = nullptr;     // max_tiles x (E+2)^3 reciprocal cell masses
     int32_t* st_nbr = nullptr;    // max_tiles x 27 neighbour indices
     // deferred / learned plasticity
     int plast_mode = PLAST_INLINE;
@@ -142,6 +143,7 @@ static cudaError_t launch_e(uint32_t edge, uint32_t kid, const Ctx& c, cudaStrea
     switch (edge) {
         case 8: return launch_kernel<8>(kid, c, s, grid, scene, apply, out);
         case 12: return launch_kernel<12>(kid, c, s, grid, scene, apply, out);
+        case 14: return launch_kernel<14>(kid, c, s, grid, scene, apply, out);
         default: return launch_kernel<16>(kid, c, s, grid, scene, apply, out);
     }
 }
@@ -317,7 +319,8 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     for (auto e : h->event_pool) cudaEventDestroy(e);
     void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
-                    h->tiles[0], h->tiles[1], h->d_scenes, h->d_scene_first, h->counters, h->iter_rec, h->st_nbr,
+                    h->tiles[0], h->tiles[1], h->tiles[2], h->tile_rm, h->d_scenes, h->d_scene_first, h->counters,
+                    h->iter_rec, h->st_nbr,
                     h->plast_list, h->d_stats, h->d_pair_count};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -361,13 +364,14 @@ static int alloc_table(MpmHandle* h, uint32_t cap) {
 }
 
 static int alloc_tiles(MpmHandle* h, uint32_t n) {
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < 3; i++)
         if (h->tiles[i]) { cudaFree(h->tiles[i]); h->tiles[i] = nullptr; }
     if (h->st_nbr) { cudaFree(h->st_nbr); h->st_nbr = nullptr; }
+    if (h->tile_rm) { cudaFree(h->tile_rm); h->tile_rm = nullptr; }
     size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     h->max_tiles = n;
-    CK(h, cudaMalloc(&h->tiles[0], (size_t)n * NC * 16));
-    CK(h, cudaMalloc(&h->tiles[1], (size_t)n * NC * 16));
+    for (int i = 0; i < 3; i++) CK(h, cudaMalloc(&h->tiles[i], (size_t)n * NC * 16));
+    CK(h, cudaMalloc(&h->tile_rm, (size_t)n * NC * 4));
     CK(h, cudaMalloc(&h->st_nbr, (size_t)n * 27 * 4));
     destroy_graphs(h);
     return MPM_OK;
@@ -381,9 +385,9 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->device = cfg->device;
     if (cfg->max_particles == 0) { *out = h; return fail(h, MPM_ERR_ARG, "max_particles must be > 0"); }
     h->tile_edge = cfg->tile_edge ? cfg->tile_edge : 16u;
-    if (h->tile_edge != 8u && h->tile_edge != 12u && h->tile_edge != 16u) {
+    if (h->tile_edge != 8u && h->tile_edge != 12u && h->tile_edge != 14u && h->tile_edge != 16u) {
         *out = h;
-        return fail(h, MPM_ERR_ARG, "tile_edge must be 8, 12 or 16");
+        return fail(h, MPM_ERR_ARG, "tile_edge must be 8, 12, 14 or 16");
     }
     uint32_t max_scenes = cfg->max_scenes ? cfg->max_scenes : 1u;
     if (max_scenes > 65534u) { *out = h; return fail(h, MPM_ERR_ARG, "max_scenes must be <= 65534"); }
@@ -438,6 +442,7 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->n_particles = 0;
     cudaError_t ce = h->tile_edge == 8u    ? configure_tile_kernels<8>(h->blocks_per_sm)
                      : h->tile_edge == 12u ? configure_tile_kernels<12>(h->blocks_per_sm)
+                     : h->tile_edge == 14u ? configure_tile_kernels<14>(h->blocks_per_sm)
                                            : configure_tile_kernels<16>(h->blocks_per_sm);
     if (ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "configure kernels: %s", cudaGetErrorString(ce));
     CK(h, cudaStreamSynchronize(h->stream));
@@ -638,6 +643,7 @@ static Ctx make_ctx(MpmHandle* h, int parity) {
     c.tiles_b = h->tiles[0];
     c.iter_rec = h->iter_rec;
     c.st_nbr = h->st_nbr;
+    c.tile_rm = h->tile_rm;
     c.plast_list = h->plast_list;
     c.plast_defer = h->plast_mode != PLAST_INLINE ? 1u : 0u;
     c.scenes = h->d_scenes;
@@ -735,18 +741,23 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
         if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = 0;
     } else {
+        // tiles[0] keeps the first transfer (with the mass sums); the
+        // iterations alternate between tiles[1] and tiles[2]
         uint32_t n_iter = h->scenes[0].params.n_iter;
         int cur = 0;
         c.tiles_a = h->tiles[cur];
         L(K_PBMPM_FIRST);
         if (stop_p2g) { h->last_tiles = cur; return cudaSuccess; }
         for (uint32_t it = 1; it < n_iter; it++) {
+            int nxt = cur == 1 ? 2 : 1;
             c.tiles_b = h->tiles[cur];
-            c.tiles_a = h->tiles[cur ^ 1];
+            c.tiles_a = h->tiles[nxt];
+            c.iter_first = it == 1 ? 1u : 0u;
             L(K_PBMPM_ITER);
-            cur ^= 1;
+            cur = nxt;
         }
         c.tiles_b = h->tiles[cur];
+        c.g2p_rm = n_iter > 1 ? 1u : 0u;
         L(K_G2P_PBMPM);
         if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = cur;
@@ -855,7 +866,8 @@ static int run_substep(MpmHandle* h, int method) {
         }
         CK(h, cudaGraphLaunch(h->graph[method][par], h->stream));
         // the captured sequence leaves its last P2G result in the same buffer
-        h->last_tiles = (method == MPM_METHOD_EXPLICIT) ? 0 : (int)((h->scenes[0].params.n_iter - 1) & 1u);
+        uint32_t ni = h->scenes[0].params.n_iter;
+        h->last_tiles = (method == MPM_METHOD_EXPLICIT || ni <= 1) ? 0 : (((ni - 1) & 1u) ? 1 : 2);
     } else {
         cudaError_t e = enqueue_substep(h, method, par, false, false);
         if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
@@ -970,6 +982,8 @@ extern "C" int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_u
     CK(h, cudaMemsetAsync(dout, 0, need * 16, h->stream));
     Ctx c = make_ctx(h, h->order_parity);
     c.tiles_b = h->tiles[h->last_tiles];
+    // the PBMPM iterations write momentum only: the mass sums are the first transfer's
+    c.tiles_m = h->last_tiles != 0 ? h->tiles[0] : nullptr;
     int grid = std::max(1, h->n_sms * std::max(1, h->blocks_per_sm[K_GRID_DENSE]));
     cudaError_t e = launch_e(h->tile_edge, K_GRID_DENSE, c, h->stream, grid, scene, apply_grid_update, dout);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out_host, dout, need * 16, cudaMemcpyDeviceToHost, h->stream);
@@ -1297,7 +1311,8 @@ constexpr size_t NA_TILES0 = NA_CHUNK_NP + na_round(NA_H / COMPACT_CHUNK * 4);  
 constexpr size_t NA_TILES1 = NA_TILES0 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
 constexpr size_t NA_ITER_REC = NA_TILES1 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);  // PBMPM records
 constexpr size_t NA_ST_NBR = NA_ITER_REC + na_round(NA_P * IR_PLANES * 16);  // tile neighbour table
-constexpr size_t NA_SCENE = NA_ST_NBR + na_round(MPM_NOALLOC_MAX_TILES * 27 * 4);
+constexpr size_t NA_RM = NA_ST_NBR + na_round(MPM_NOALLOC_MAX_TILES * 27 * 4);   // reciprocal cell masses
+constexpr size_t NA_SCENE = NA_RM + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 4);
 constexpr size_t NA_SCENE_FIRST = NA_SCENE + na_round(sizeof(SceneDev));
 constexpr size_t NA_COUNTERS = NA_SCENE_FIRST + na_round(2 * 4);
 constexpr size_t NA_BYTES = NA_COUNTERS + na_round(sizeof(Counters));
@@ -1426,6 +1441,7 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     c.tiles_b = tiles[0];
     c.iter_rec = (float4*)(b + NA_ITER_REC);
     c.st_nbr = (int32_t*)(b + NA_ST_NBR);
+    c.tile_rm = (float*)(b + NA_RM);
     c.scenes = (const SceneDev*)(b + NA_SCENE);
     c.scene_first = (const uint32_t*)(b + NA_SCENE_FIRST);
     c.counters = (Counters*)(b + NA_COUNTERS);
@@ -1464,10 +1480,12 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
         for (uint32_t it = 1; it < params->n_iter; it++) {
             c.tiles_b = tiles[cur];
             c.tiles_a = tiles[cur ^ 1];
+            c.iter_first = it == 1 ? 1u : 0u;
             NA_CK(run(K_PBMPM_ITER));
             cur ^= 1;
         }
         c.tiles_b = tiles[cur];
+        c.g2p_rm = params->n_iter > 1 ? 1u : 0u;
         NA_CK(run(K_G2P_PBMPM));
     }
     if (status_out) {

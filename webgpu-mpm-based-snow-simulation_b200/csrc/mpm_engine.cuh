@@ -11,15 +11,18 @@
 //   slot_count  cap x u32  particles per slot
 //   slot_off, slot_st      per-slot particle offset and compact tile index
 //   st_key/st_slot/st_begin/st_count   per compact tile
-//   tiles[2]    max_tiles x (E+2)^3 x int4   per-tile halo sums
-//               (mass, momentum x, y, z) in the reference i32 fixed point
+//   tiles[3]    max_tiles x (E+2)^3 x int4   per-tile halo sums
+//               (mass, momentum x, y, z) in the reference i32 fixed point;
+//               the PBMPM iterations write momentum only (mass field 0)
+//   tile_rm     max_tiles x (E+2)^3 f32      reciprocal cell masses of the
+//               substep, formed by its first PBMPM iteration
 //   iter_rec    IR_PLANES x N float4         PBMPM iteration records (below)
 //   st_nbr      max_tiles x 27 i32           compact index of each tile's 27
 //                                            neighbours (d = 9(dz+1) + 3(dy+1) + dx+1),
 //                                            built once per substep after binning
 //
-// A tile is E^3 grid cells (E = 8, 12 or 16, i.e. 2^3, 3^3 or 4^3 of the reference's
-// 4^3-cell blocks).  Its P2G writes the (E+2)^3 halo region it touches; the
+// A tile is E^3 grid cells (E = 8, 12, 14 or 16; 8, 12 and 16 are 2^3, 3^3 and 4^3 of
+// the reference's 4^3-cell blocks).  Its P2G writes the (E+2)^3 halo region it touches; the
 // grid value of a cell is the i32 sum over every tile halo that covers it
 // (at most 8), formed on the fly by the G2P kernels.  Integer addition
 // commutes, so the sums equal the reference's atomicAdd totals exactly.
@@ -120,6 +123,10 @@ struct Ctx {
     int4* tiles_b;            // tiles read by this pass's G2P
     float4* iter_rec;         // PBMPM iteration records, IR_PLANES x n float4, sorted order
     int32_t* st_nbr;          // per compact tile, the compact index of its 27 neighbours (-1: none)
+    float* tile_rm;           // per tile (E+2)^3 reciprocal cell masses of the substep (PBMPM iterations)
+    const int4* tiles_m;      // readback only: tiles holding the substep's mass sums (nullptr: tiles_b)
+    uint32_t iter_first;      // this PBMPM iteration forms and stores the reciprocal masses
+    uint32_t g2p_rm;          // the final PBMPM G2P reads the stored reciprocal masses
     uint32_t* plast_list;     // deferred plasticity: particles the strain-bound check did not clear
     uint32_t plast_defer;     // 0: exact return map inside integrate; 1: deferred to the plasticity pass
     const SceneDev* scenes;

@@ -832,11 +832,12 @@ __host__ __device__ constexpr HaloTable<E> make_halo_table() {
 
 __device__ const HaloTable<8> g_halo8 = make_halo_table<8>();
 __device__ const HaloTable<12> g_halo12 = make_halo_table<12>();
+__device__ const HaloTable<14> g_halo14 = make_halo_table<14>();
 __device__ const HaloTable<16> g_halo16 = make_halo_table<16>();
 
 template <int E>
 __device__ __forceinline__ const uint32_t* halo_table() {
-    return E == 8 ? g_halo8.v : (E == 12 ? g_halo12.v : g_halo16.v);
+    return E == 8 ? g_halo8.v : (E == 12 ? g_halo12.v : (E == 14 ? g_halo14.v : g_halo16.v));
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
@@ -850,11 +851,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // parts of the neighbour halos (entries of the compile-time halo table,
 // loaded into registers in batches of U per thread and added with shared
 // i32 atomics).  The first batch of neighbour loads is issued before the
-// wait for the copies, so both latencies overlap.  COPY_MASS also keeps this
-// tile's own halo mass sums in own_mass (before the neighbour sums land).
-template <int E, int BS, bool COPY_MASS = false>
-__device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr, int4* cell,
-                                              uint32_t* own_mass = nullptr) {
+// wait for the copies, so both latencies overlap.  MASS = false adds only
+// the momentum components (the mass field of the result is then undefined).
+template <int E, int BS, bool MASS = true>
+__device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr, int4* cell) {
     constexpr int H = E + 2, NC = H * H * H;
     constexpr int NE = HaloEntries<E>::N;
     constexpr int PER = (NE + BS - 1) / BS;      // entries per thread
@@ -885,7 +885,7 @@ __device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr,
         for (int u = 0; u < U; u++) {
             if (jd[u] >= 0) {
                 int* dst = reinterpret_cast<int*>(&cell[jd[u]]);
-                atomicAdd(dst + 0, v[u].x);
+                if (MASS) atomicAdd(dst + 0, v[u].x);
                 atomicAdd(dst + 1, v[u].y);
                 atomicAdd(dst + 2, v[u].z);
                 atomicAdd(dst + 3, v[u].w);
@@ -895,10 +895,6 @@ __device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr,
     fetch(threadIdx.x);
     cp_async_wait_all();
     __syncthreads();
-    if (COPY_MASS) {
-        for (int j = threadIdx.x; j < NC; j += BS) own_mass[j] = (uint32_t)cell[j].x;
-        __syncthreads();
-    }
     add();
     for (int base = threadIdx.x + U * BS; base < NE; base += U * BS) {
         fetch(base);
@@ -906,18 +902,78 @@ __device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr,
     }
 }
 
+// Reciprocal cell mass RN(1 / m) of the velocity m^-1 p, 0 for the cells the
+// reference skips (outside the grid or mass <= 0): a momentum scaled by 0
+// gives a velocity of +-0, whose products add nothing to the G2P sums.
+__device__ __forceinline__ float mass_recip(const SceneDev& S, int32_t m, const int* gc) {
+    bool in = gc[0] >= 0 && gc[1] >= 0 && gc[2] >= 0 && gc[0] < S.res[0] && gc[1] < S.res[1] && gc[2] < S.res[2];
+    float cm = inv_s(S, m);
+    return (in && cm > 0.0f) ? __frcp_rn(cm) : 0.0f;
+}
+
+// PBMPM cell velocity from momentum and the reciprocal mass (gridToParticle.cs.wgsl:102-108)
+__device__ __forceinline__ float4 cell_velocity_rm(const SceneDev& S, int4 s, float rm, const int* gc) {
+    float v[3] = {fm(inv_s(S, s.y), rm), fm(inv_s(S, s.z), rm), fm(inv_s(S, s.w), rm)};
+    grid_bc(S, gc, v);
+    return make_float4(v[0], v[1], v[2], 0.f);
+}
+
 // Assemble this tile's (E+2)^3 cell velocities in shared memory: halo sums
-// (assemble_sums), then each sum turned into the velocity in place.
-template <int E, int BS, bool PB, bool COPY_MASS = false>
+// (assemble_sums), then each sum turned into the velocity in place.  RM
+// selects where the cell masses come from: 0, the assembled mass sums (the
+// reference path, explicit grid update included); 1, the same, and the
+// reciprocal masses are also stored to rm_tile for later passes of the
+// substep; 2, the reciprocal masses stored by such a pass (the halo sums then
+// carry momentum only).
+template <int E, int BS, bool PB, int RM = 0>
 __device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
-                                                       const int* nbr, int4* cell, uint32_t* own_mass = nullptr) {
+                                                       const int* nbr, int4* cell, float* rm_tile = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
-    assemble_sums<E, BS, COPY_MASS>(tiles, nbr, cell, own_mass);
+    constexpr int KC = (NC + BS - 1) / BS;   // cells per thread
+    // Stored reciprocal masses go into the mass field of the sums (unused in
+    // momentum-only mode) before the conversion.  With few cells per thread
+    // all loads are issued before the assembly, so their latency overlaps
+    // it; otherwise after it, in batches (no register spills).
+    constexpr bool EARLY = KC <= 12;
+    float rmv[(RM == 2 && EARLY) ? KC : 1];
+    if (RM == 2 && EARLY) {
+#pragma unroll
+        for (int k = 0; k < KC; k++) {
+            int j = threadIdx.x + k * BS;
+            rmv[k] = j < NC ? __ldg(rm_tile + j) : 0.0f;
+        }
+    }
+    assemble_sums<E, BS, RM != 2>(tiles, nbr, cell);
+    if (RM == 2) {
+        if (EARLY) {
+#pragma unroll
+            for (int k = 0; k < KC; k++) {
+                int j = threadIdx.x + k * BS;
+                if (j < NC) cell[j].x = __float_as_int(rmv[k]);
+            }
+        } else {
+#pragma unroll 8
+            for (int j = threadIdx.x; j < NC; j += BS) cell[j].x = __float_as_int(__ldg(rm_tile + j));
+        }
+    }
     __syncthreads();
     for (int j = threadIdx.x; j < NC; j += BS) {
         int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
         int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
-        float4 v = cell_velocity<PB>(S, cell[j], gc);
+        float4 v;
+        int4 sm = cell[j];
+        if (RM == 0) {
+            v = cell_velocity<PB>(S, sm, gc);
+        } else {
+            float rm;
+            if (RM == 1) {
+                rm = mass_recip(S, sm.x, gc);
+                rm_tile[j] = rm;
+            } else {
+                rm = __int_as_float(sm.x);
+            }
+            v = cell_velocity_rm(S, sm, rm, gc);
+        }
         reinterpret_cast<float4*>(cell)[j] = v;
     }
 }
@@ -1098,7 +1154,7 @@ __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const Tile
                     float aff = ff(D[6 + k], off[2][oz], pxy[k]);
                     uint32_t v = (uint32_t)enc_rdt<FOLD>(S, fm(wm, fa(dxp[k], aff)));
                     if (fon[k]) v += (uint32_t)enc_dt<FOLD>(S, fm(fo[k], wm));
-                    atomicAdd(cell + (k + 1) * NC, v);
+                    atomicAdd(cell + (k + (WITH_MASS ? 1 : 0)) * NC, v);
                 }
                 if (WITH_MASS) atomicAdd(cell, (uint32_t)f2i(fm(wm, S.scale)));
             }
@@ -1119,10 +1175,19 @@ __device__ __forceinline__ void flush_tile(uint32_t* acc, int4* dst) {
         dst[j] = make_int4((int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j], (int)acc[3 * NC + j]);
 }
 
+// momentum-only accumulator of the PBMPM iterations: 3 planes x (E+2)^3
 template <int E>
 __device__ __forceinline__ void zero_mom(uint32_t* acc) {
     constexpr int H = E + 2, NC = H * H * H;
-    for (int j = threadIdx.x; j < 3 * NC; j += blockDim.x) acc[NC + j] = 0u;
+    uint4* a4 = reinterpret_cast<uint4*>(acc);
+    for (int j = threadIdx.x; j < 3 * NC / 4; j += blockDim.x) a4[j] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+template <int E>
+__device__ __forceinline__ void flush_mom(const uint32_t* acc, int4* dst) {
+    constexpr int H = E + 2, NC = H * H * H;
+    for (int j = threadIdx.x; j < NC; j += blockDim.x)
+        dst[j] = make_int4(0, (int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j]);
 }
 
 template <int E>
@@ -1237,7 +1302,7 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
 // G2P + integrate (explicit: gridToParticle.cs.wgsl:28-80; PBMPM :82-130;
 // integrateParticles.wgsl:14-72)
 // ------------------------------------------------------------------
-template <int E, bool PB, int BS>
+template <int E, bool PB, int BS, int RM = 0>
 __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
     extern __shared__ uint4 smem_raw[];
     int4* cell = reinterpret_cast<int4*>(smem_raw);
@@ -1251,7 +1316,8 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
         __syncthreads();
-        assemble_velocity_tile<E, BS, PB>(c.tiles_b, S, T, nbr, cell);
+        constexpr int NCT = (E + 2) * (E + 2) * (E + 2);
+        assemble_velocity_tile<E, BS, PB, RM>(c.tiles_b, S, T, nbr, cell, c.tile_rm + (size_t)st * NCT);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1335,14 +1401,19 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
 }
 
 // PBMPM iteration i>0: G2P of iteration i-1, constraints, P2G of iteration i,
-// all from the iteration records (contiguous in tile order)
-template <int E, int BS>
+// all from the iteration records (contiguous in tile order).  Positions and
+// masses are fixed within a substep, so the cell masses are the first
+// transfer's: the first iteration (FIRST) forms their reciprocals from the
+// mass sums and stores them; later iterations read them back, and every
+// iteration accumulates and writes momentum only.  Shared memory: the halo
+// sums / velocities (16 B per cell) and three momentum planes (12 B per cell).
+template <int E, int BS, bool FIRST>
 __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
     extern __shared__ uint4 smem_raw[];
-    uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
-    int4* cell = reinterpret_cast<int4*>(smem_raw + NC);
-    const float4* vel = reinterpret_cast<const float4*>(smem_raw + NC);
+    int4* cell = reinterpret_cast<int4*>(smem_raw);
+    const float4* vel = reinterpret_cast<const float4*>(smem_raw);
+    uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw + NC);
     __shared__ SceneDev S;
     __shared__ int nbr[27];
     uint32_t cur_scene = INVALID;
@@ -1353,7 +1424,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
         load_neighbors(c, st, nbr);
         zero_mom<E>(acc);
         __syncthreads();
-        assemble_velocity_tile<E, BS, true, true>(c.tiles_b, S, T, nbr, cell, acc);
+        assemble_velocity_tile<E, BS, true, FIRST ? 1 : 2>(c.tiles_b, S, T, nbr, cell, c.tile_rm + (size_t)st * NC);
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1368,7 +1439,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
             p2g_pbmpm<E, false>(S, T, sc, mass, dxp, D, acc);
         }
         __syncthreads();
-        flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
+        flush_mom<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
 }
@@ -1392,6 +1463,7 @@ __global__ void __launch_bounds__(256) k_grid_dense(Ctx c, uint32_t scene, int a
         __syncthreads();
         for (int j = threadIdx.x; j < NC; j += blockDim.x) {
             int4 s = assemble_cell<E>(c.tiles_b, nbr, j);
+            if (c.tiles_m) s.x = assemble_cell<E>(c.tiles_m, nbr, j).x;
             int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
             int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
             if (gc[0] < 0 || gc[1] < 0 || gc[2] < 0 || gc[0] >= S.res[0] || gc[1] >= S.res[1] || gc[2] >= S.res[2]) continue;
@@ -1473,7 +1545,7 @@ size_t smem_bytes(uint32_t kid) {
         case K_PBMPM_FIRST:
         case K_G2P_EXPLICIT:
         case K_G2P_PBMPM: return 16 * NC;
-        case K_PBMPM_ITER: return 32 * NC;
+        case K_PBMPM_ITER: return 28 * NC;
         default: return 0;
     }
 }
@@ -1486,32 +1558,44 @@ int block_size(uint32_t kid) {
     return kid == K_PBMPM_ITER ? iter_block<E>() : BS_DEFAULT;
 }
 
+// every instantiation behind a kernel id (variants share the id's launch shape)
 template <int E>
-void* kernel_ptr(uint32_t kid) {
+int kernel_ptrs(uint32_t kid, void** out) {
     switch (kid) {
-        case K_BIN_INSERT: return (void*)k_bin_insert<E>;
-        case K_P2G_EXPLICIT: return (void*)k_p2g_explicit<E, BS_DEFAULT>;
-        case K_G2P_EXPLICIT: return (void*)k_g2p_integrate<E, false, BS_DEFAULT>;
-        case K_PBMPM_FIRST: return (void*)k_pbmpm_first<E, BS_DEFAULT>;
-        case K_PBMPM_ITER: return (void*)k_pbmpm_iter<E, iter_block<E>()>;
-        case K_G2P_PBMPM: return (void*)k_g2p_integrate<E, true, BS_DEFAULT>;
-        case K_GRID_DENSE: return (void*)k_grid_dense<E>;
-        case K_TILE_NBR: return (void*)k_tile_nbr<E>;
-        default: return nullptr;
+        case K_BIN_INSERT: out[0] = (void*)k_bin_insert<E>; return 1;
+        case K_P2G_EXPLICIT: out[0] = (void*)k_p2g_explicit<E, BS_DEFAULT>; return 1;
+        case K_G2P_EXPLICIT: out[0] = (void*)k_g2p_integrate<E, false, BS_DEFAULT, 0>; return 1;
+        case K_PBMPM_FIRST: out[0] = (void*)k_pbmpm_first<E, BS_DEFAULT>; return 1;
+        case K_PBMPM_ITER:
+            out[0] = (void*)k_pbmpm_iter<E, iter_block<E>(), true>;
+            out[1] = (void*)k_pbmpm_iter<E, iter_block<E>(), false>;
+            return 2;
+        case K_G2P_PBMPM:
+            out[0] = (void*)k_g2p_integrate<E, true, BS_DEFAULT, 2>;
+            out[1] = (void*)k_g2p_integrate<E, true, BS_DEFAULT, 0>;
+            return 2;
+        case K_GRID_DENSE: out[0] = (void*)k_grid_dense<E>; return 1;
+        case K_TILE_NBR: out[0] = (void*)k_tile_nbr<E>; return 1;
+        default: return 0;
     }
 }
 
 template <int E>
 cudaError_t configure_tile_kernels(int* blocks_per_sm) {
     for (uint32_t kid : {K_P2G_EXPLICIT, K_G2P_EXPLICIT, K_PBMPM_FIRST, K_PBMPM_ITER, K_G2P_PBMPM, K_GRID_DENSE}) {
-        void* f = kernel_ptr<E>(kid);
+        void* fs[2] = {nullptr, nullptr};
+        int nf = kernel_ptrs<E>(kid, fs);
         size_t sm = smem_bytes<E>(kid);
-        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        int nb = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, f, block_size<E>(kid), sm);
-        if (e != cudaSuccess) return e;
-        blocks_per_sm[kid] = nb > 0 ? nb : 1;
+        int nb_min = 1 << 30;
+        for (int i = 0; i < nf; i++) {
+            cudaError_t e = cudaFuncSetAttribute(fs[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return e;
+            int nb = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fs[i], block_size<E>(kid), sm);
+            if (e != cudaSuccess) return e;
+            nb_min = nb < nb_min ? nb : nb_min;
+        }
+        blocks_per_sm[kid] = nb_min > 0 ? nb_min : 1;
     }
     return cudaSuccess;
 }
@@ -1531,10 +1615,16 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
         case K_BIN_SCATTER: if (pblocks) k_bin_scatter<<<pblocks, 256, 0, s>>>(c); break;
         case K_TILE_NBR: k_tile_nbr<E><<<grid_tiles, 256, 0, s>>>(c); break;
         case K_P2G_EXPLICIT: k_p2g_explicit<E, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
-        case K_G2P_EXPLICIT: k_g2p_integrate<E, false, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
+        case K_G2P_EXPLICIT: k_g2p_integrate<E, false, BS_DEFAULT, 0><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
         case K_PBMPM_FIRST: k_pbmpm_first<E, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
-        case K_PBMPM_ITER: k_pbmpm_iter<E, iter_block<E>()><<<grid_tiles, iter_block<E>(), smem_bytes<E>(kid), s>>>(c); break;
-        case K_G2P_PBMPM: k_g2p_integrate<E, true, BS_DEFAULT><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c); break;
+        case K_PBMPM_ITER:
+            if (c.iter_first) k_pbmpm_iter<E, iter_block<E>(), true><<<grid_tiles, iter_block<E>(), smem_bytes<E>(kid), s>>>(c);
+            else k_pbmpm_iter<E, iter_block<E>(), false><<<grid_tiles, iter_block<E>(), smem_bytes<E>(kid), s>>>(c);
+            break;
+        case K_G2P_PBMPM:
+            if (c.g2p_rm) k_g2p_integrate<E, true, BS_DEFAULT, 2><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c);
+            else k_g2p_integrate<E, true, BS_DEFAULT, 0><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c);
+            break;
         case K_GRID_DENSE: k_grid_dense<E><<<grid_tiles, 256, 0, s>>>(c, scene, apply, out); break;
         default: return cudaErrorInvalidValue;
     }
@@ -1548,9 +1638,11 @@ cudaError_t launch_selftest(uint64_t n, uint64_t seed, unsigned long long* count
 
 template cudaError_t configure_tile_kernels<8>(int*);
 template cudaError_t configure_tile_kernels<12>(int*);
+template cudaError_t configure_tile_kernels<14>(int*);
 template cudaError_t configure_tile_kernels<16>(int*);
 template cudaError_t launch_kernel<8>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
 template cudaError_t launch_kernel<12>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
+template cudaError_t launch_kernel<14>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
 template cudaError_t launch_kernel<16>(uint32_t, const Ctx&, cudaStream_t, int, uint32_t, int, int4*);
 
 }  // namespace mpm

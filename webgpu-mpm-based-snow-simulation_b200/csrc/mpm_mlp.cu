@@ -44,9 +44,17 @@ __device__ __forceinline__ void st_row8(uint8_t* base, uint32_t r, uint32_t k0, 
     *reinterpret_cast<uint4*>(base + tc::kmaj(r, k0, R)) = q;
 }
 
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z / 2)) / 2 with the hardware tanh (one MUFU
+// operation per element instead of an exponential and a reciprocal)
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float silu_grad(float z) {
-    float s = __fdividef(1.0f, 1.0f + __expf(-z));
+    float s = sigmoid(z);
     return s + z * s * (1.0f - s);
 }
 
