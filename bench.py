@@ -504,6 +504,39 @@ def batched_leg(pkg, args, local, stream):
             "batched_vs_loop": loop_ms / ms, "unit": "particle-substeps/s"}
 
 
+def mlp_case(local):
+    """The network alone (the profiling case of its kernels): forward passes over
+    1,048,576 random rows and one training epoch over 65,536 random pairs;
+    prints the forward throughput."""
+    import numpy as np
+    import torch
+
+    pkg = importlib.import_module(PKG)
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    net = pkg.learned.PlasticityNet(device=local, seed=1)
+    net.set_stream(stream.cuda_stream)
+    rng = np.random.default_rng(0)
+    n = 1 << 20
+    x = torch.from_numpy(rng.normal(0, 1, (n, 12)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.normal(0, 1, (n, 10)).astype(np.float32)).cuda()
+    for _ in range(3):
+        net.forward(x)
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    for _ in range(5):
+        net.forward(x)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    net.train(x[:65536].contiguous(), t[:65536].contiguous(), epochs=1, batch=8192)
+    torch.cuda.synchronize()
+    flops = 2.0 * (12 * 64 + 64 * 64 * 2 + 64 * 11) * n
+    print(json.dumps({"case": "mlp", "rows": n, "forward_ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}), flush=True)
+    net.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,6 +545,8 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--tile-edge", type=int, default=16)
     ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--mlp-case", action="store_true",
+                    help="run only the learned-plasticity network on random rows (profiling case of its kernels)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the learned-plasticity and batched-scene legs (they run at N = 1 only)")
     ap.add_argument("--counts", default="256,64,256",
@@ -519,6 +554,9 @@ def main():
                          "lattices give the small cases used for profiling)")
     args = ap.parse_args()
     args.counts = tuple(int(v) for v in args.counts.split(","))
+    if args.mlp_case:
+        mlp_case(dist_env()[2])
+        return
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
 

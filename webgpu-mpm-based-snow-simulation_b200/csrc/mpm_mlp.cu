@@ -32,8 +32,8 @@ namespace {
 constexpr uint32_t WAIT_LIMIT = 1u << 22;   // mbarrier polls before a pass gives up
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
-           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);   // one conversion for two values, a in the low half
+    return *reinterpret_cast<uint32_t*>(&h);
 }
 __device__ __forceinline__ void st_bf16(uint8_t* base, uint32_t off, float v) {
     *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
