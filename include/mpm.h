@@ -51,6 +51,7 @@ extern "C" {
 #define MPM_STATUS_SCENE_RANGE    0x8u  /* a particle index belongs to no scene */
 #define MPM_STATUS_MLP_FALLBACK   0x10u /* learned plasticity fell back to the exact map */
 #define MPM_STATUS_MLP_TIMEOUT    0x20u /* a tensor-core wait of the plasticity pass ran out */
+#define MPM_STATUS_COPY_TIMEOUT   0x40u /* a halo bulk-copy wait of a tile kernel ran out */
 
 typedef struct MpmHandle MpmHandle;
 

@@ -22,6 +22,7 @@ STATUS_BITS = {
     0x8: "particle outside every scene range",
     0x10: "learned plasticity fallback",
     0x20: "learned plasticity tensor-core wait ran out",
+    0x40: "halo bulk-copy wait ran out",
 }
 
 PLASTICITY_INLINE = 0

@@ -53,6 +53,7 @@ constexpr uint32_t ST_BVH_STACK = 0x4u;
 constexpr uint32_t ST_SCENE_RANGE = 0x8u;
 constexpr uint32_t ST_MLP_FALLBACK = 0x10u;
 constexpr uint32_t ST_MLP_TIMEOUT = 0x20u;
+constexpr uint32_t ST_COPY_TIMEOUT = 0x40u;
 
 
 // Per-scene parameters: the uniform fields the step reads plus the

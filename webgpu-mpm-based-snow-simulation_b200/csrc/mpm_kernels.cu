@@ -840,28 +840,76 @@ __device__ __forceinline__ const uint32_t* halo_table() {
     return E == 8 ? g_halo8.v : (E == 12 ? g_halo12.v : (E == 14 ? g_halo14.v : g_halo16.v));
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-    uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+// ---- TMA bulk copies into shared memory, completing on an mbarrier ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init1(uint64_t* mbar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+                 : "memory");
+}
+// waits for the phase of the given parity; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t* mbar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(mbar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+constexpr uint32_t COPY_WAIT_LIMIT = 1u << 22;
 
-// Sum this tile's halo region into `cell`: the tile's own (E+2)^3 sums
-// (asynchronous 16-byte copies, all in flight at once) plus the overlapping
-// parts of the neighbour halos (entries of the compile-time halo table,
-// loaded into registers in batches of U per thread and added with shared
-// i32 atomics).  The first batch of neighbour loads is issued before the
-// wait for the copies, so both latencies overlap.  MASS = false adds only
-// the momentum components (the mass field of the result is then undefined).
+// Per-CTA state of the halo copies of the tile kernels: the mbarrier the
+// bulk copies complete on and the parity of its current phase.
+struct HaloCopy {
+    uint64_t* mbar;
+    uint32_t parity;
+};
+
+// Sum this tile's halo region into `cell`: the tile's own (E+2)^3 sums (one
+// TMA bulk copy) plus the overlapping parts of the neighbour halos (entries
+// of the compile-time halo table, loaded into registers in batches of U per
+// thread and added with shared i32 atomics).  The first batch of neighbour
+// loads is issued before the wait for the bulk copy, so both latencies
+// overlap.  rm_src / rm_dst (optional): the tile's stored reciprocal masses,
+// brought in by the same bulk copy.  MASS = false adds only the momentum
+// components (the mass field of the result is then undefined).  Returns false
+// (on every thread) when the copy wait ran out; the caller then stops.
 template <int E, int BS, bool MASS = true>
-__device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr, int4* cell) {
+__device__ __forceinline__ bool assemble_sums(const int4* tiles, const int* nbr, int4* cell, HaloCopy& hc,
+                                              const float* rm_src = nullptr, float* rm_dst = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
     constexpr int NE = HaloEntries<E>::N;
     constexpr int PER = (NE + BS - 1) / BS;      // entries per thread
     constexpr int U = PER <= 10 ? PER : 8;       // entries per register batch
     const int4* own = tiles + (size_t)nbr[13] * NC;
     const uint32_t* tab = halo_table<E>();
-    for (int j = threadIdx.x; j < NC; j += BS) cp_async16(&cell[j], own + j);
+    if (threadIdx.x == 0) {
+        // the previous tile's shared-memory reads (generic proxy) come before these writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(hc.mbar, (uint32_t)(NC * 16 + (rm_dst ? NC * 4 : 0)));
+        constexpr uint32_t CH = (NC * 16) / 4 / 16 * 16;   // four chunks, 16-byte multiples
+        bulk_g2s(cell, own, CH, hc.mbar);
+        bulk_g2s(reinterpret_cast<char*>(cell) + CH, reinterpret_cast<const char*>(own) + CH, CH, hc.mbar);
+        bulk_g2s(reinterpret_cast<char*>(cell) + 2 * CH, reinterpret_cast<const char*>(own) + 2 * CH, CH, hc.mbar);
+        bulk_g2s(reinterpret_cast<char*>(cell) + 3 * CH, reinterpret_cast<const char*>(own) + 3 * CH,
+                 (uint32_t)(NC * 16) - 3 * CH, hc.mbar);
+        if (rm_dst) bulk_g2s(rm_dst, rm_src, (uint32_t)(NC * 4), hc.mbar);
+    }
     int4 v[U];
     int jd[U];
     auto fetch = [&](int base) {
@@ -893,13 +941,15 @@ __device__ __forceinline__ void assemble_sums(const int4* tiles, const int* nbr,
         }
     };
     fetch(threadIdx.x);
-    cp_async_wait_all();
-    __syncthreads();
+    bool ok = mbar_wait_parity(hc.mbar, hc.parity, COPY_WAIT_LIMIT);
+    hc.parity ^= 1u;
+    if (__syncthreads_or(ok ? 0 : 1)) return false;
     add();
     for (int base = threadIdx.x + U * BS; base < NE; base += U * BS) {
         fetch(base);
         add();
     }
+    return true;
 }
 
 // Reciprocal cell mass RN(1 / m) of the velocity m^-1 p, 0 for the cells the
@@ -924,58 +974,61 @@ __device__ __forceinline__ float4 cell_velocity_rm(const SceneDev& S, int4 s, fl
 // reference path, explicit grid update included); 1, the same, and the
 // reciprocal masses are also stored to rm_tile for later passes of the
 // substep; 2, the reciprocal masses stored by such a pass (the halo sums then
-// carry momentum only).
+// carry momentum only), brought into rm_s by the halo's bulk copy when rm_s
+// is given, else loaded after the assembly into the unused mass field.
+// Returns false (on every thread) when the halo copy wait ran out.
 template <int E, int BS, bool PB, int RM = 0>
-__device__ __forceinline__ void assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
-                                                       const int* nbr, int4* cell, float* rm_tile = nullptr) {
+__device__ __forceinline__ bool assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
+                                                       const int* nbr, int4* cell, HaloCopy& hc,
+                                                       float* rm_tile = nullptr, float* rm_s = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
-    constexpr int KC = (NC + BS - 1) / BS;   // cells per thread
-    // Stored reciprocal masses go into the mass field of the sums (unused in
-    // momentum-only mode) before the conversion.  With few cells per thread
-    // all loads are issued before the assembly, so their latency overlaps
-    // it; otherwise after it, in batches (no register spills).
-    constexpr bool EARLY = KC <= 12;
-    float rmv[(RM == 2 && EARLY) ? KC : 1];
-    if (RM == 2 && EARLY) {
-#pragma unroll
-        for (int k = 0; k < KC; k++) {
-            int j = threadIdx.x + k * BS;
-            rmv[k] = j < NC ? __ldg(rm_tile + j) : 0.0f;
-        }
-    }
-    assemble_sums<E, BS, RM != 2>(tiles, nbr, cell);
-    if (RM == 2) {
-        if (EARLY) {
-#pragma unroll
-            for (int k = 0; k < KC; k++) {
-                int j = threadIdx.x + k * BS;
-                if (j < NC) cell[j].x = __float_as_int(rmv[k]);
-            }
-        } else {
+    const bool rm_bulk = RM == 2 && rm_s != nullptr;
+    if (!assemble_sums<E, BS, RM != 2>(tiles, nbr, cell, hc, rm_bulk ? rm_tile : nullptr,
+                                       rm_bulk ? rm_s : nullptr))
+        return false;
+    if (RM == 2 && !rm_bulk) {
 #pragma unroll 8
-            for (int j = threadIdx.x; j < NC; j += BS) cell[j].x = __float_as_int(__ldg(rm_tile + j));
-        }
+        for (int j = threadIdx.x; j < NC; j += BS) cell[j].x = __float_as_int(__ldg(rm_tile + j));
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < NC; j += BS) {
-        int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
-        int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
-        float4 v;
-        int4 sm = cell[j];
-        if (RM == 0) {
-            v = cell_velocity<PB>(S, sm, gc);
-        } else {
-            float rm;
-            if (RM == 1) {
-                rm = mass_recip(S, sm.x, gc);
-                rm_tile[j] = rm;
-            } else {
-                rm = __int_as_float(sm.x);
-            }
-            v = cell_velocity_rm(S, sm, rm, gc);
+    // batches of CB cells per thread: all loads, then all conversions, then
+    // all stores, so the cells' dependency chains overlap
+    constexpr int CB = (BS >= 512 && RM != 0) ? 4 : 1;
+    for (int j0 = threadIdx.x; j0 < NC; j0 += CB * BS) {
+        int4 sm[CB];
+        float rmu[CB];
+#pragma unroll
+        for (int u = 0; u < CB; u++) {
+            int j = j0 + u * BS;
+            sm[u] = j < NC ? cell[j] : make_int4(0, 0, 0, 0);
+            rmu[u] = (RM == 2 && j < NC) ? (rm_bulk ? rm_s[j] : __int_as_float(sm[u].x)) : 0.0f;
         }
-        reinterpret_cast<float4*>(cell)[j] = v;
+        float4 v[CB];
+#pragma unroll
+        for (int u = 0; u < CB; u++) {
+            int j = j0 + u * BS;
+            int lx = j % H, ly = (j / H) % H, lz = j / (H * H);
+            int gc[3] = {T.origin[0] - 1 + lx, T.origin[1] - 1 + ly, T.origin[2] - 1 + lz};
+            if (RM == 0) {
+                v[u] = cell_velocity<PB>(S, sm[u], gc);
+            } else {
+                float rm;
+                if (RM == 1) {
+                    rm = mass_recip(S, sm[u].x, gc);
+                    if (j < NC) rm_tile[j] = rm;
+                } else {
+                    rm = rmu[u];
+                }
+                v[u] = cell_velocity_rm(S, sm[u], rm, gc);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < CB; u++) {
+            int j = j0 + u * BS;
+            if (j < NC) reinterpret_cast<float4*>(cell)[j] = v[u];
+        }
     }
+    return true;
 }
 
 // G2P gather from the shared velocity tile (gridToParticle.cs.wgsl:28-130).
@@ -1186,6 +1239,7 @@ __device__ __forceinline__ void zero_mom(uint32_t* acc) {
 template <int E>
 __device__ __forceinline__ void flush_mom(const uint32_t* acc, int4* dst) {
     constexpr int H = E + 2, NC = H * H * H;
+#pragma unroll 4
     for (int j = threadIdx.x; j < NC; j += blockDim.x)
         dst[j] = make_int4(0, (int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j]);
 }
@@ -1195,6 +1249,17 @@ __device__ __forceinline__ void zero_acc(uint32_t* acc) {
     constexpr int H = E + 2, NC = H * H * H;
     uint4* a4 = reinterpret_cast<uint4*>(acc);
     for (int j = threadIdx.x; j < NC; j += blockDim.x) a4[j] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// A halo copy wait ran out: report it, give the copy in flight a second
+// bounded wait (so no bulk write lands after the CTA has exited), and let the
+// caller return.
+__device__ __noinline__ void copy_wait_failed(const Ctx& c, HaloCopy& hc) {
+    if (threadIdx.x == 0) {
+        atomicOr(&c.counters->status, ST_COPY_TIMEOUT);
+        mbar_wait_parity(hc.mbar, hc.parity ^ 1u, COPY_WAIT_LIMIT);
+    }
+    __syncthreads();
 }
 
 __device__ __forceinline__ uint32_t n_tiles_now(const Ctx& c) {
@@ -1309,6 +1374,10 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
     const float4* vel = reinterpret_cast<const float4*>(smem_raw);
     __shared__ SceneDev S;
     __shared__ int nbr[27];
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) mbar_init1(&mbar);
+    __syncthreads();
+    HaloCopy hc{&mbar, 0u};
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
     for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
@@ -1317,7 +1386,10 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
         load_neighbors(c, st, nbr);
         __syncthreads();
         constexpr int NCT = (E + 2) * (E + 2) * (E + 2);
-        assemble_velocity_tile<E, BS, PB, RM>(c.tiles_b, S, T, nbr, cell, c.tile_rm + (size_t)st * NCT);
+        if (!assemble_velocity_tile<E, BS, PB, RM>(c.tiles_b, S, T, nbr, cell, hc, c.tile_rm + (size_t)st * NCT)) {
+            copy_wait_failed(c, hc);
+            return;
+        }
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1414,8 +1486,13 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     int4* cell = reinterpret_cast<int4*>(smem_raw);
     const float4* vel = reinterpret_cast<const float4*>(smem_raw);
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw + NC);
+    float* rm_s = reinterpret_cast<float*>(acc + 3 * NC);   // stored reciprocal masses (later iterations)
     __shared__ SceneDev S;
     __shared__ int nbr[27];
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) mbar_init1(&mbar);
+    __syncthreads();
+    HaloCopy hc{&mbar, 0u};
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
     for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
@@ -1424,7 +1501,11 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
         load_neighbors(c, st, nbr);
         zero_mom<E>(acc);
         __syncthreads();
-        assemble_velocity_tile<E, BS, true, FIRST ? 1 : 2>(c.tiles_b, S, T, nbr, cell, c.tile_rm + (size_t)st * NC);
+        if (!assemble_velocity_tile<E, BS, true, FIRST ? 1 : 2>(c.tiles_b, S, T, nbr, cell, hc,
+                                                               c.tile_rm + (size_t)st * NC, FIRST ? nullptr : rm_s)) {
+            copy_wait_failed(c, hc);
+            return;
+        }
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
@@ -1545,7 +1626,7 @@ size_t smem_bytes(uint32_t kid) {
         case K_PBMPM_FIRST:
         case K_G2P_EXPLICIT:
         case K_G2P_PBMPM: return 16 * NC;
-        case K_PBMPM_ITER: return 28 * NC;
+        case K_PBMPM_ITER: return 32 * NC;
         default: return 0;
     }
 }
