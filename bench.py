@@ -272,6 +272,25 @@ def gpu_run(args, rank, world, local):
     torch.cuda.synchronize()
     ex_rate = n * ex_steps / (e0.elapsed_time(e1) * 1e-3)
 
+    # ---- renderer splats of the final state (calculateGridMass.wgsl, mcDensity.cs.wgsl)
+    rx, ry, rz = spec.res
+    mass_grid = torch.zeros((rz, ry, rx), dtype=torch.int32, device="cuda")
+    dens_grid = torch.zeros((rz // 2, ry // 2, rx // 2), dtype=torch.int32, device="cuda")
+    splats = {}
+    for name, fn in (("grid_mass", lambda: buf.calculate_grid_mass(spec.res, out=mass_grid)),
+                     ("mc_density", lambda: buf.calculate_density((rx // 2, ry // 2, rz // 2), out=dens_grid))):
+        fn()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(5):
+            fn()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ms_s = s0.elapsed_time(s1) / 5
+        splats[name] = {"ms": round(ms_s, 4), "particles_per_s": n / (ms_s * 1e-3)}
+    del mass_grid, dens_grid
+
     # ---- end to end through the public API with host buffers
     host = torch.empty(n * 192, dtype=torch.uint8, pin_memory=True)
     import numpy as np
@@ -325,6 +344,7 @@ def gpu_run(args, rank, world, local):
         "p2g_gbs": round(p2g_gbs, 1),
         "g2p_gbs": round(g2p_gbs, 1),
         "explicit_value": ex_rate,
+        "splats": splats,
         "kernels": {k: round(v["ms_per_launch"], 4) for k, v in kernels.items()},
         "e2e": {"value": e2e_rate, "unit": "particle-substeps/s", "h2d_bytes_per_step": n * 192,
                 "d2h_bytes_per_step": n * 192},

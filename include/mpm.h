@@ -174,6 +174,19 @@ int mpm_use_graphs(MpmHandle* h, int enable);
 int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* ident_mismatches, uint64_t* cvt_mismatches,
                  uint64_t* nan_conversion);
 
+/* ---- renderer splats ------------------------------------------------ */
+/* The particle splats the reference's renderers run after the step, into the
+ * caller's device buffer of u32 (res_x * res_y * res_z, x fastest), enqueued
+ * on the handle's stream; accumulate = 0 clears the buffer first.
+ * mpm_grid_mass: calculateGridMass (src/lib/gpu/volumetric/calculateGridMass.wgsl:8-51),
+ *   on the scene's simulation grid (uniform gridResolution).
+ * mpm_mc_density: calculateDensity (src/lib/gpu/marchingCubes/mcDensity.cs.wgsl:14-63),
+ *   on a density grid of density_res[3] cells over the same domain (the
+ *   reference uses half the simulation resolution,
+ *   src/lib/gpu/marchingCubes/GpuMarchingCubesBufferManager.ts:44-48). */
+int mpm_grid_mass(MpmHandle* h, uint32_t scene, uint32_t* out_dev, int accumulate);
+int mpm_mc_density(MpmHandle* h, uint32_t scene, const uint32_t* density_res, uint32_t* out_dev, int accumulate);
+
 /* ---- learned plasticity --------------------------------------------
  * The snow return map applyPlasticity (src/lib/gpu/shaderPrelude/
  * plasticityOps.wgsl:7-48, called from integrateParticles.wgsl) can run in

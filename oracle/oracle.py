@@ -1,5 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU oracle (liboracle.so,
-built from mpm_oracle.c / bvh_oracle.c by oracle/Makefile).
+built from mpm_oracle.c / bvh_oracle.c / mlp_oracle.c / splat_oracle.c by
+oracle/Makefile).
 
 The oracle restates the reference MPM step (WGSL under src/lib/gpu/mpm/ and
 src/lib/gpu/shaderPrelude/, scheduled by GpuMpmPipelineManager.ts:327-521).
@@ -21,7 +22,8 @@ UNIFORMS_BYTES = 37376
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "mlp_oracle.c", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "mlp_oracle.c", "splat_oracle.c",
+                                             "Makefile")]
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return LIB
@@ -73,6 +75,8 @@ def lib():
             "or_mlp_features": (I32, [V, V, C.c_float, C.c_float, V]),
             "or_mlp_targets": (None, [V, V, V, V, V]),
             "or_cert_elastic": (I32, [C.c_float, C.c_float, V]),
+            "or_grid_mass": (None, [V, U32, V, V, V, C.c_float, V]),
+            "or_mc_density": (None, [V, U32, V, V, V, C.c_float, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -232,3 +236,18 @@ def cert_elastic(Fe, theta_c, theta_s):
     fe = np.ascontiguousarray(Fe, np.float32).reshape(9)
     smin, smax = np.float32(1.0 - float(np.float32(theta_c))), np.float32(1.0 + float(np.float32(theta_s)))
     return bool(lib().or_cert_elastic(float(smin), float(smax), fe.ctypes.data))
+
+
+# ---- renderer splats (splat_oracle.c) ---------------------------------
+def splat(kind, records, grid_min, grid_max, res, scale):
+    """calculateGridMass (kind 'mass') or calculateDensity (kind 'density'):
+    u32 grid [res_z][res_y][res_x]."""
+    rec = np.ascontiguousarray(records)
+    gmin = np.ascontiguousarray(grid_min, np.float32)
+    gmax = np.ascontiguousarray(grid_max, np.float32)
+    r = np.ascontiguousarray(res, np.uint32)
+    out = np.zeros((int(r[2]), int(r[1]), int(r[0])), np.uint32)
+    f = lib().or_grid_mass if kind == "mass" else lib().or_mc_density
+    f(rec.ctypes.data, rec.shape[0], gmin.ctypes.data, gmax.ctypes.data, r.ctypes.data, float(np.float32(scale)),
+      out.ctypes.data)
+    return out

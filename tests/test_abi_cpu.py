@@ -74,9 +74,10 @@ def test_create_fails_cleanly_without_gpu_or_bad_args(pkg):
     assert rc != 0
     assert b"max_particles" in lib.mpm_last_error(h)
     lib.mpm_destroy(h)
-    cfg = pkg.MpmConfig(max_particles=10, max_scenes=1, tile_edge=12)
+    cfg = pkg.MpmConfig(max_particles=10, max_scenes=1, tile_edge=13)
     rc = lib.mpm_create(C.byref(cfg), C.byref(h))
     assert rc != 0
+    assert b"tile_edge" in lib.mpm_last_error(h)
     lib.mpm_destroy(h)
 
 

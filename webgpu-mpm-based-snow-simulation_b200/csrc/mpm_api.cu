@@ -26,6 +26,15 @@ template <int E> cudaError_t configure_tile_kernels(int* blocks_per_sm);
 template <int E> cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_tiles, uint32_t scene,
                                            int apply, int4* out);
 cudaError_t launch_selftest(uint64_t n, uint64_t seed, unsigned long long* counts, cudaStream_t s);
+struct SplatArgs {
+    const float4* particles;
+    uint32_t first, count;
+    float gmin[3], gmax[3];
+    uint32_t res[3];
+    float scale;
+    uint32_t* out;
+};
+cudaError_t launch_splat(int kind, const SplatArgs& a, cudaStream_t s);
 }  // namespace mpm
 
 using namespace mpm;
@@ -991,6 +1000,46 @@ extern "C" int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_u
     cudaFree(dout);
     if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "grid readback: %s", cudaGetErrorString(e));
     return MPM_OK;
+}
+
+// Particle splats for the renderers (calculateGridMass.wgsl, mcDensity.cs.wgsl):
+// enqueued on the handle's stream into the caller's device buffer.
+static int splat(MpmHandle* h, uint32_t scene, int kind, const uint32_t* res, uint32_t* out_dev, int accumulate) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (scene >= h->n_scenes) return fail(h, MPM_ERR_ARG, "scene %u >= scene count", scene);
+    if (!out_dev) return fail(h, MPM_ERR_ARG, "null output buffer");
+    cudaSetDevice(h->device);
+    r = upload_scenes(h);
+    if (r) return r;
+    const SceneDev& d = h->scenes[scene].dev;
+    SplatArgs a{};
+    a.particles = h->particles;
+    a.first = d.p_first;
+    a.count = d.p_count;
+    for (int k = 0; k < 3; k++) {
+        a.gmin[k] = d.gmin[k];
+        a.gmax[k] = d.gmax[k];
+        a.res[k] = res ? res[k] : (uint32_t)d.res[k];
+        if (a.res[k] == 0) return fail(h, MPM_ERR_ARG, "splat resolution must be > 0");
+    }
+    a.scale = d.scale;
+    a.out = out_dev;
+    if (!accumulate)
+        CK(h, cudaMemsetAsync(out_dev, 0, (size_t)a.res[0] * a.res[1] * a.res[2] * 4, h->stream));
+    CK(h, launch_splat(kind, a, h->stream));
+    return MPM_OK;
+}
+
+extern "C" int mpm_grid_mass(MpmHandle* h, uint32_t scene, uint32_t* out_dev, int accumulate) {
+    if (!h) return MPM_ERR_ARG;
+    return splat(h, scene, 0, nullptr, out_dev, accumulate);
+}
+
+extern "C" int mpm_mc_density(MpmHandle* h, uint32_t scene, const uint32_t* density_res, uint32_t* out_dev,
+                              int accumulate) {
+    if (!h || !density_res) return MPM_ERR_ARG;
+    return splat(h, scene, 1, density_res, out_dev, accumulate);
 }
 
 extern "C" int mpm_enable_kernel_timing(MpmHandle* h, int enable) {

@@ -95,6 +95,7 @@ class GpuMpmBufferManager:
             raise _lib.MpmError(rc, msg)
         self.n_particles = n_particles
         self.tile_edge = tile_edge
+        self.device = device
         self._lib = lib
 
     def close(self) -> None:
@@ -139,6 +140,27 @@ class GpuMpmBufferManager:
         a, b = C.c_uint32(0), C.c_uint32(0)
         check(self._lib.mpm_get_counts(self.handle, C.byref(a), C.byref(b)), self.handle)
         return a.value, b.value
+
+    def calculate_grid_mass(self, res, scene: int = 0, out=None):
+        """calculateGridMass (GpuVolumetricRenderPipelineManager.ts): the mass
+        splat on the simulation grid, a torch u32-as-int32 CUDA tensor [z][y][x]."""
+        import torch
+
+        rx, ry, rz = (int(r) for r in res)
+        out = torch.zeros((rz, ry, rx), dtype=torch.int32, device=f"cuda:{self.device}") if out is None else out
+        check(self._lib.mpm_grid_mass(self.handle, scene, C.c_void_p(out.data_ptr()), 0), self.handle)
+        return out
+
+    def calculate_density(self, density_res, scene: int = 0, out=None):
+        """calculateDensity (GpuMarchingCubesRenderPipelineManager.ts): the
+        marching-cubes density splat, a torch u32-as-int32 CUDA tensor [z][y][x]."""
+        import torch
+
+        rx, ry, rz = (int(r) for r in density_res)
+        out = torch.zeros((rz, ry, rx), dtype=torch.int32, device=f"cuda:{self.device}") if out is None else out
+        res = (C.c_uint32 * 3)(rx, ry, rz)
+        check(self._lib.mpm_mc_density(self.handle, scene, res, C.c_void_p(out.data_ptr()), 0), self.handle)
+        return out
 
     def dense_grid(self, res, scene: int = 0, apply_grid_update: bool = False) -> np.ndarray:
         rx, ry, rz = (int(r) for r in res)
