@@ -290,6 +290,20 @@ def gpu_run(args, rank, world, local):
         ms_s = s0.elapsed_time(s1) / 5
         splats[name] = {"ms": round(ms_s, 4), "particles_per_s": n / (ms_s * 1e-3)}
     del mass_grid, dens_grid
+    # ---- particle initialisation (scatterParticles) into a 1,280-triangle icosphere, 262,144 particles
+    v_ico, f_ico = pkg.scenes.icosphere(3, 0.15, (0.5, 0.5, 0.5))
+    mesh = pkg.GpuMeshBufferManager(vertices=v_ico, indices=f_ico)
+    sbuf = pkg.GpuMpmBufferManager(n_particles=262144, device=local, stream=stream.cuda_stream)
+    sinit = pkg.GpuParticleInitializePipelineManager(mpm_manager=sbuf, mesh_manager=mesh,
+                                                     uniforms_manager=pkg.GpuUniformsBufferManager())
+    sinit.add_dispatch(n_particles=262144)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    sinit.add_dispatch(n_particles=262144)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    splats["scatter_particles"] = {"ms": round(s0.elapsed_time(s1), 4), "particles": 262144, "triangles": 1280}
+    sbuf.close()
 
     # ---- end to end through the public API with host buffers
     host = torch.empty(n * 192, dtype=torch.uint8, pin_memory=True)

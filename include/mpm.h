@@ -174,6 +174,16 @@ int mpm_use_graphs(MpmHandle* h, int enable);
 int mpm_selftest(int device, uint64_t n, uint64_t seed, uint64_t* ident_mismatches, uint64_t* cvt_mismatches,
                  uint64_t* nan_conversion);
 
+/* ---- particle initialisation --------------------------------------- */
+/* scatterParticles (src/lib/gpu/particleInitialize/particleScatter.cs.wgsl:47-84):
+ * fills the handle's first n_particles records with positions drawn inside
+ * the closed triangle mesh (rejection sampling in the box given by scene
+ * 0's uniform meshMinCoords / meshMaxCoords, even-odd ray parity, at most 512
+ * attempts), fBm-jittered, with hashed masses and rest state.  vertices: host
+ * triangle soup, n_vertices x 4 floats (x, y, z, unused), as the reference's
+ * mesh vertex buffer (GpuMeshBufferManager.ts:30-43).  Synchronous. */
+int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32_t n_vertices, uint32_t n_particles);
+
 /* ---- renderer splats ------------------------------------------------ */
 /* The particle splats the reference's renderers run after the step, into the
  * caller's device buffer of u32 (res_x * res_y * res_z, x fastest), enqueued

@@ -1,6 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU oracle (liboracle.so,
-built from mpm_oracle.c / bvh_oracle.c / mlp_oracle.c / splat_oracle.c by
-oracle/Makefile).
+built from mpm_oracle.c / bvh_oracle.c / mlp_oracle.c / splat_oracle.c /
+scatter_oracle.c by oracle/Makefile).
 
 The oracle restates the reference MPM step (WGSL under src/lib/gpu/mpm/ and
 src/lib/gpu/shaderPrelude/, scheduled by GpuMpmPipelineManager.ts:327-521).
@@ -23,7 +23,7 @@ UNIFORMS_BYTES = 37376
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "mlp_oracle.c", "splat_oracle.c",
-                                             "Makefile")]
+                                             "scatter_oracle.c", "Makefile")]
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return LIB
@@ -77,6 +77,7 @@ def lib():
             "or_cert_elastic": (I32, [C.c_float, C.c_float, V]),
             "or_grid_mass": (None, [V, U32, V, V, V, C.c_float, V]),
             "or_mc_density": (None, [V, U32, V, V, V, C.c_float, V]),
+            "or_scatter": (None, [V, U32, V, V, U32, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -250,4 +251,15 @@ def splat(kind, records, grid_min, grid_max, res, scale):
     f = lib().or_grid_mass if kind == "mass" else lib().or_mc_density
     f(rec.ctypes.data, rec.shape[0], gmin.ctypes.data, gmax.ctypes.data, r.ctypes.data, float(np.float32(scale)),
       out.ctypes.data)
+    return out
+
+
+# ---- particle scatter (scatter_oracle.c) --------------------------------
+def scatter(vertices4, mesh_min, mesh_max, n):
+    """scatterParticles: n 192-byte records (as raw bytes reshaped [n, 192])."""
+    v = np.ascontiguousarray(vertices4, np.float32)
+    mn = np.ascontiguousarray(mesh_min, np.float32)
+    mx = np.ascontiguousarray(mesh_max, np.float32)
+    out = np.zeros((n, 192), np.uint8)
+    lib().or_scatter(v.ctypes.data, v.shape[0] // 3, mn.ctypes.data, mx.ctypes.data, n, out.ctypes.data)
     return out

@@ -9,12 +9,14 @@ generators.
 from . import _lib, batching, layout, learned, scenes
 from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams, default_params, load
 from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
-from .pipeline import (GpuColliderBufferManager, GpuMpmBatch, GpuMpmBufferManager, GpuMpmPipelineManager,
-                       GpuSimulationMethodType, build_bvh, kernel_names)
+from .pipeline import (GpuColliderBufferManager, GpuMeshBufferManager, GpuMpmBatch, GpuMpmBufferManager,
+                       GpuMpmPipelineManager, GpuParticleInitializePipelineManager, GpuSimulationMethodType, build_bvh,
+                       kernel_names)
 
 __all__ = [
     "METHOD_EXPLICIT", "METHOD_PBMPM", "MpmConfig", "MpmError", "MpmParams", "default_params", "load",
     "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
-    "GpuMpmBufferManager", "GpuMpmBatch", "GpuMpmPipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
+    "GpuMpmBufferManager", "GpuMpmBatch", "GpuMpmPipelineManager", "GpuMeshBufferManager",
+    "GpuParticleInitializePipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
     "layout", "scenes", "learned", "batching",
 ]

@@ -128,6 +128,7 @@ SIGNATURES = {
     "mpm_use_graphs": (C.c_int, [_H, C.c_int]),
     "mpm_selftest": (C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                C.POINTER(C.c_uint64)]),
+    "mpm_scatter_particles": (C.c_int, [_H, C.c_void_p, C.c_uint32, C.c_uint32]),
     "mpm_grid_mass": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_int]),
     "mpm_mc_density": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]),
     "mpm_mlp_init_params": (C.c_int, [C.c_uint32, C.c_void_p]),

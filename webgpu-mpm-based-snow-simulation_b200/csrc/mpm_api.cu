@@ -35,6 +35,14 @@ struct SplatArgs {
     uint32_t* out;
 };
 cudaError_t launch_splat(int kind, const SplatArgs& a, cudaStream_t s);
+struct ScatterArgs {
+    float4* particles;
+    uint32_t n;
+    const float4* verts;
+    uint32_t n_tris;
+    float mmin[3], mmax[3];
+};
+cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t s);
 }  // namespace mpm
 
 using namespace mpm;
@@ -1040,6 +1048,37 @@ extern "C" int mpm_mc_density(MpmHandle* h, uint32_t scene, const uint32_t* dens
                               int accumulate) {
     if (!h || !density_res) return MPM_ERR_ARG;
     return splat(h, scene, 1, density_res, out_dev, accumulate);
+}
+
+extern "C" int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32_t n_vertices, uint32_t n_particles) {
+    if (!h) return MPM_ERR_ARG;
+    if (!vertices || n_vertices < 3 || n_vertices % 3 != 0)
+        return fail(h, MPM_ERR_ARG, "vertices must be a triangle soup of 3k vertices");
+    if (n_particles > h->cfg.max_particles)
+        return fail(h, MPM_ERR_CAPACITY, "%u particles exceed max_particles %u", n_particles, h->cfg.max_particles);
+    if (!h->own_particles) return fail(h, MPM_ERR_STATE, "particle buffer is bound to caller memory");
+    cudaSetDevice(h->device);
+    int r = set_count(h, n_particles);
+    if (r) return r;
+    ScatterArgs a{};
+    a.particles = h->particles;
+    a.n = n_particles;
+    a.n_tris = n_vertices / 3;
+    const uint8_t* u = h->scenes[0].uni;   // uniforms.meshMinCoords @176, meshMaxCoords @192
+    for (int k = 0; k < 3; k++) {
+        a.mmin[k] = rdf(u, 176 + 4 * k);
+        a.mmax[k] = rdf(u, 192 + 4 * k);
+    }
+    float4* dv = nullptr;
+    CK(h, cudaMalloc(&dv, (size_t)n_vertices * 16));
+    a.verts = dv;
+    cudaError_t e = cudaMemcpyAsync(dv, vertices, (size_t)n_vertices * 16, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = launch_scatter(a, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dv);
+    if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "scatter: %s", cudaGetErrorString(e));
+    h->order_valid = false;
+    return MPM_OK;
 }
 
 extern "C" int mpm_enable_kernel_timing(MpmHandle* h, int enable) {

@@ -47,6 +47,27 @@ __host__ __device__ __forceinline__ uint32_t hash3(uint32_t x, uint32_t y, uint3
     return h ^ (h >> 16);
 }
 
+// 1- and 4-word variants of the same mix (randomNumberGenerators.wgsl:3-9, 40-55)
+__host__ __device__ __forceinline__ uint32_t hash1(uint32_t n) {
+    uint32_t h = n + 374761393u;
+    h = 668265263u * ((h << 17) | (h >> 15));
+    h = 2246822519u * (h ^ (h >> 15));
+    h = 3266489917u * (h ^ (h >> 13));
+    return h ^ (h >> 16);
+}
+__host__ __device__ __forceinline__ uint32_t hash4(uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+    const uint32_t p2 = 2246822519u, p3 = 3266489917u, p4 = 668265263u, p5 = 374761393u;
+    uint32_t h = w + p5 + x * p3;
+    h = p4 * ((h << 17) | (h >> 15));
+    h += y * p3;
+    h = p4 * ((h << 17) | (h >> 15));
+    h += z * p3;
+    h = p4 * ((h << 17) | (h >> 15));
+    h = p2 * (h ^ (h >> 15));
+    h = p3 * (h ^ (h >> 13));
+    return h ^ (h >> 16);
+}
+
 // exp(x) in f64: Cody-Waite reduction x = k ln2 + r, then the degree-13
 // Taylor polynomial of e^r (Horner), then exact scaling by 2^k.
 __device__ __forceinline__ double pow2i(int k) {

@@ -230,6 +230,43 @@ class GpuMpmPipelineManager:
         check(self._lib.mpm_step(self.mpm.handle, int(method), n_substeps), self.mpm.handle)
 
 
+class GpuMeshBufferManager:
+    """The closed mesh particles are scattered into (GpuMeshBufferManager.ts:1-46):
+    a triangle soup of vertices padded to 4 floats, and its bounding box."""
+
+    def __init__(self, *, vertices, indices=None):
+        v = np.asarray(vertices, np.float32).reshape(-1, 3)
+        if indices is not None:
+            v = v[np.asarray(indices, np.int64).reshape(-1)]
+        self.vertices = np.zeros((v.shape[0], 4), np.float32)
+        self.vertices[:, :3] = v
+        self.num_vertices = v.shape[0]
+        self.min_coords = v.min(0)
+        self.max_coords = v.max(0)
+
+
+class GpuParticleInitializePipelineManager:
+    """scatterParticles (GpuParticleInitializePipelineManager.ts:88-104):
+    writes the mesh box into the uniforms and fills the particle buffer."""
+
+    def __init__(self, *, mpm_manager: GpuMpmBufferManager, mesh_manager: GpuMeshBufferManager,
+                 uniforms_manager: GpuUniformsBufferManager):
+        self.mpm = mpm_manager
+        self.mesh = mesh_manager
+        self.uniforms = uniforms_manager
+        self._lib = load()
+
+    def add_dispatch(self, *, n_particles: int) -> None:
+        self.uniforms.write_mesh_min_coords(self.mesh.min_coords)
+        self.uniforms.write_mesh_max_coords(self.mesh.max_coords)
+        b = self.uniforms.bytes()
+        check(self._lib.mpm_set_uniforms(self.mpm.handle, 0, b, len(b)), self.mpm.handle)
+        v = self.mesh.vertices
+        check(self._lib.mpm_scatter_particles(self.mpm.handle, v.ctypes.data, v.shape[0], n_particles),
+              self.mpm.handle)
+        self.mpm.n_particles = n_particles
+
+
 class GpuMpmBatch:
     """Many independent scenes advanced by the same launches: one handle, one
     scene table, particles concatenated in scene order.  Each scene keeps its
