@@ -289,7 +289,27 @@ def gpu_run(args, rank, world, local):
         torch.cuda.synchronize()
         ms_s = s0.elapsed_time(s1) / 5
         splats[name] = {"ms": round(ms_s, 4), "particles_per_s": n / (ms_s * 1e-3)}
-    del mass_grid, dens_grid
+    del dens_grid
+    # ---- volumetric ray march of the final state (volumetricRaymarch.cs.wgsl), 1280 x 720
+    rw, rh = 1280, 720
+    spec.uniforms.write_view_proj_inv_mat(pkg.scenes.camera_inv_view_proj((0.5, -0.9, 1.2), (0.5, 0.5, 0.3), rw, rh))
+    spec.uniforms.write_time(1)
+    pipe.push_uniforms()
+    vol = pkg.GpuVolumetricBufferManager(grid_resolution=spec.res, screen_dims=(rw, rh), device=local,
+                                         mass_grid=mass_grid)
+    rpipe = pkg.GpuVolumetricRenderPipelineManager(mpm_manager=buf, volumetric_manager=vol)
+    rpipe.add_raymarch_dispatch()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(3):
+        rpipe.add_raymarch_dispatch()
+    s1.record(stream)
+    torch.cuda.synchronize()
+    ms_r = s0.elapsed_time(s1) / 3
+    splats["volumetric_raymarch"] = {"ms": round(ms_r, 4), "pixels": rw * rh,
+                                     "covered": int((vol.output[..., 3] > 0).sum().item())}
+    del vol, rpipe, mass_grid
     # ---- particle initialisation (scatterParticles) into a 1,280-triangle icosphere, 262,144 particles
     v_ico, f_ico = pkg.scenes.icosphere(3, 0.15, (0.5, 0.5, 0.5))
     mesh = pkg.GpuMeshBufferManager(vertices=v_ico, indices=f_ico)

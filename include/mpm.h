@@ -197,6 +197,20 @@ int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32_t n_vertic
 int mpm_grid_mass(MpmHandle* h, uint32_t scene, uint32_t* out_dev, int accumulate);
 int mpm_mc_density(MpmHandle* h, uint32_t scene, const uint32_t* density_res, uint32_t* out_dev, int accumulate);
 
+/* ---- volumetric ray march ------------------------------------------- */
+/* doVolumetricRaymarch (src/lib/gpu/volumetric/volumetricRaymarch.cs.wgsl:118-226,
+ * dispatched by GpuVolumetricRenderPipelineManager.addRaymarchDispatch,
+ * GpuVolumetricRenderPipelineManager.ts:332-339) into headless device buffers
+ * instead of the storage textures: rgba_dev width*height*4 bytes (rgba8unorm,
+ * round to nearest), depth_dev width*height f32 (r32float; left unwritten
+ * where the ray misses the grid, as the texture is), color_dev optional
+ * width*height*4 f32 (the stored vec4f before quantisation).  mass_grid_dev is
+ * the scene's calculateGridMass grid (mpm_grid_mass); the camera is the
+ * uniform block's viewProjInvMat (@112) and the jitter seed its time (@12).
+ * Enqueued on the handle's stream; 1 <= width, height <= 16384. */
+int mpm_volumetric_raymarch(MpmHandle* h, uint32_t scene, const uint32_t* mass_grid_dev, uint32_t width,
+                            uint32_t height, uint8_t* rgba_dev, float* depth_dev, float* color_dev);
+
 /* ---- learned plasticity --------------------------------------------
  * The snow return map applyPlasticity (src/lib/gpu/shaderPrelude/
  * plasticityOps.wgsl:7-48, called from integrateParticles.wgsl) can run in

@@ -23,7 +23,7 @@ UNIFORMS_BYTES = 37376
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "mlp_oracle.c", "splat_oracle.c",
-                                             "scatter_oracle.c", "Makefile")]
+                                             "scatter_oracle.c", "raymarch_oracle.c", "Makefile")]
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return LIB
@@ -78,6 +78,7 @@ def lib():
             "or_grid_mass": (None, [V, U32, V, V, V, C.c_float, V]),
             "or_mc_density": (None, [V, U32, V, V, V, C.c_float, V]),
             "or_scatter": (None, [V, U32, V, V, U32, V]),
+            "or_raymarch": (None, [V, V, V, V, C.c_float, V, U32, U32, U32, V, V, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -263,3 +264,24 @@ def scatter(vertices4, mesh_min, mesh_max, n):
     out = np.zeros((n, 192), np.uint8)
     lib().or_scatter(v.ctypes.data, v.shape[0] // 3, mn.ctypes.data, mx.ctypes.data, n, out.ctypes.data)
     return out
+
+
+# ---- volumetric ray march (raymarch_oracle.c) ---------------------------
+def raymarch(mass_grid, grid_min, grid_max, scale, inv_view_proj, time, width, height, depth_init=None):
+    """doVolumetricRaymarch over a width x height image: (rgba [h][w][4] u8,
+    depth [h][w] f32, color [h][w][4] f32).  mass_grid is the u32
+    calculateGridMass grid [res_z][res_y][res_x]; inv_view_proj the 16
+    column-major floats of viewProjInvMat."""
+    m = np.ascontiguousarray(mass_grid, np.uint32)
+    res = np.array([m.shape[2], m.shape[1], m.shape[0]], np.uint32)
+    gmin = np.ascontiguousarray(grid_min, np.float32)
+    gmax = np.ascontiguousarray(grid_max, np.float32)
+    M = np.ascontiguousarray(np.asarray(inv_view_proj, np.float32).reshape(16))
+    rgba = np.zeros((height, width, 4), np.uint8)
+    depth = (np.full((height, width), np.float32(-1.0), np.float32) if depth_init is None
+             else np.ascontiguousarray(depth_init, np.float32).copy())
+    color = np.zeros((height, width, 4), np.float32)
+    lib().or_raymarch(m.ctypes.data, res.ctypes.data, gmin.ctypes.data, gmax.ctypes.data, float(np.float32(scale)),
+                      M.ctypes.data, int(time), int(width), int(height), rgba.ctypes.data, depth.ctypes.data,
+                      color.ctypes.data)
+    return rgba, depth, color

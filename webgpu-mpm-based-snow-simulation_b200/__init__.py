@@ -10,13 +10,14 @@ from . import _lib, batching, layout, learned, scenes
 from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams, default_params, load
 from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
 from .pipeline import (GpuColliderBufferManager, GpuMeshBufferManager, GpuMpmBatch, GpuMpmBufferManager,
-                       GpuMpmPipelineManager, GpuParticleInitializePipelineManager, GpuSimulationMethodType, build_bvh,
-                       kernel_names)
+                       GpuMpmPipelineManager, GpuParticleInitializePipelineManager, GpuSimulationMethodType,
+                       GpuVolumetricBufferManager, GpuVolumetricRenderPipelineManager, build_bvh, kernel_names)
 
 __all__ = [
     "METHOD_EXPLICIT", "METHOD_PBMPM", "MpmConfig", "MpmError", "MpmParams", "default_params", "load",
     "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
     "GpuMpmBufferManager", "GpuMpmBatch", "GpuMpmPipelineManager", "GpuMeshBufferManager",
-    "GpuParticleInitializePipelineManager", "GpuSimulationMethodType", "build_bvh", "kernel_names",
+    "GpuParticleInitializePipelineManager", "GpuSimulationMethodType", "GpuVolumetricBufferManager",
+    "GpuVolumetricRenderPipelineManager", "build_bvh", "kernel_names",
     "layout", "scenes", "learned", "batching",
 ]

@@ -1050,6 +1050,42 @@ extern "C" int mpm_mc_density(MpmHandle* h, uint32_t scene, const uint32_t* dens
     return splat(h, scene, 1, density_res, out_dev, accumulate);
 }
 
+// Volumetric ray march (volumetricRaymarch.cs.wgsl): camera and time from the
+// scene's uniform block (viewProjInvMat @112, time @12), grid bounds,
+// resolution and fixed-point scale from its parameters.
+extern "C" int mpm_volumetric_raymarch(MpmHandle* h, uint32_t scene, const uint32_t* mass_grid_dev, uint32_t width,
+                                       uint32_t height, uint8_t* rgba_dev, float* depth_dev, float* color_dev) {
+    if (!h) return MPM_ERR_ARG;
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (scene >= h->n_scenes) return fail(h, MPM_ERR_ARG, "scene %u >= scene count", scene);
+    if (!mass_grid_dev || !rgba_dev || !depth_dev) return fail(h, MPM_ERR_ARG, "null buffer");
+    if (width == 0 || height == 0 || width > 16384 || height > 16384)
+        return fail(h, MPM_ERR_ARG, "image size %ux%u outside 1..16384", width, height);
+    cudaSetDevice(h->device);
+    r = upload_scenes(h);
+    if (r) return r;
+    const SceneDev& d = h->scenes[scene].dev;
+    const uint8_t* u = h->scenes[scene].uni;
+    RaymarchArgs a{};
+    a.mass = mass_grid_dev;
+    for (int k = 0; k < 3; k++) {
+        a.res[k] = (uint32_t)d.res[k];
+        a.gmin[k] = d.gmin[k];
+        a.gmax[k] = d.gmax[k];
+    }
+    a.scale = d.scale;
+    for (int k = 0; k < 16; k++) a.inv_vp[k] = rdf(u, 112 + 4 * k);
+    a.time = rdu(u, 12);
+    a.width = width;
+    a.height = height;
+    a.rgba = rgba_dev;
+    a.depth = depth_dev;
+    a.color = color_dev;
+    CK(h, launch_raymarch(a, h->stream));
+    return MPM_OK;
+}
+
 extern "C" int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32_t n_vertices, uint32_t n_particles) {
     if (!h) return MPM_ERR_ARG;
     if (!vertices || n_vertices < 3 || n_vertices % 3 != 0)

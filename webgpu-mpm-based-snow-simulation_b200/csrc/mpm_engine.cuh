@@ -95,6 +95,21 @@ struct SceneDev {
 };
 static_assert(sizeof(SceneDev) % 8 == 0, "SceneDev must be 8-byte sized");
 
+// Arguments of the volumetric ray march (mpm_raymarch.cu).
+struct RaymarchArgs {
+    const uint32_t* mass;   // res[0] * res[1] * res[2] u32, x fastest (calculateGridMass output)
+    uint32_t res[3];
+    float gmin[3], gmax[3];
+    float scale;            // fixedPointScale
+    float inv_vp[16];       // viewProjInvMat, column-major
+    uint32_t time;
+    uint32_t width, height;
+    uint8_t* rgba;          // width * height * 4 (rgba8unorm)
+    float* depth;           // width * height (r32float)
+    float* color;           // optional width * height * 4: the stored vec4f before quantisation
+};
+cudaError_t launch_raymarch(const RaymarchArgs& a, cudaStream_t s);
+
 struct Counters {
     uint32_t n_st;       // occupied tiles of the current substep
     uint32_t n_binned;   // particles placed in tiles

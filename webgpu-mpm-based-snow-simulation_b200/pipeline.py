@@ -267,6 +267,72 @@ class GpuParticleInitializePipelineManager:
         self.mpm.n_particles = n_particles
 
 
+class GpuVolumetricBufferManager:
+    """Device buffers of the volumetric renderer (GpuVolumetricBufferManager.ts:1-74),
+    headless: the u32 mass grid on the simulation grid, the rgba8unorm output
+    image and the r32float depth image as torch CUDA tensors, plus the f32
+    colour before quantisation."""
+
+    def __init__(self, *, grid_resolution, screen_dims, device: int = 0, mass_grid=None):
+        """mass_grid: an existing int32 CUDA tensor [z][y][x] to render from
+        (e.g. the result of GpuMpmBufferManager.calculate_grid_mass)."""
+        import torch
+
+        self.grid_resolution = tuple(int(r) for r in grid_resolution)
+        self.device = device
+        rx, ry, rz = self.grid_resolution
+        dev = f"cuda:{device}"
+        if mass_grid is not None and tuple(mass_grid.shape) != (rz, ry, rx):
+            raise ValueError(f"mass grid shape {tuple(mass_grid.shape)} != {(rz, ry, rx)}")
+        self.mass_grid = torch.zeros((rz, ry, rx), dtype=torch.int32, device=dev) if mass_grid is None else mass_grid
+        self._alloc(*screen_dims)
+
+    def _alloc(self, width: int, height: int) -> None:
+        import torch
+
+        dev = f"cuda:{self.device}"
+        self.width, self.height = int(width), int(height)
+        self.output = torch.zeros((self.height, self.width, 4), dtype=torch.uint8, device=dev)
+        self.depth = torch.zeros((self.height, self.width), dtype=torch.float32, device=dev)
+        self.color = torch.zeros((self.height, self.width, 4), dtype=torch.float32, device=dev)
+
+    def resize(self, width: int, height: int) -> None:
+        self._alloc(width, height)
+
+
+class GpuVolumetricRenderPipelineManager:
+    """The volumetric renderer's compute passes (GpuVolumetricRenderPipelineManager.ts:325-356):
+    clear the mass grid, calculateGridMass, doVolumetricRaymarch, all on the
+    handle's stream.  The composite draw (a full-screen triangle strip) has no
+    headless counterpart: the output image is the result."""
+
+    def __init__(self, *, mpm_manager: GpuMpmBufferManager, volumetric_manager: GpuVolumetricBufferManager,
+                 scene: int = 0):
+        self.mpm = mpm_manager
+        self.vol = volumetric_manager
+        self.scene = scene
+        self._lib = load()
+
+    def add_mass_calculation_dispatch(self, clear: bool = True) -> None:
+        """calculateGridMass; clear=True also clears the grid first, on the same
+        stream (the pass's clearBuffer)."""
+        check(self._lib.mpm_grid_mass(self.mpm.handle, self.scene, C.c_void_p(self.vol.mass_grid.data_ptr()),
+                                      0 if clear else 1), self.mpm.handle)
+
+    def add_raymarch_dispatch(self) -> None:
+        v = self.vol
+        check(self._lib.mpm_volumetric_raymarch(self.mpm.handle, self.scene, C.c_void_p(v.mass_grid.data_ptr()),
+                                                v.width, v.height, C.c_void_p(v.output.data_ptr()),
+                                                C.c_void_p(v.depth.data_ptr()), C.c_void_p(v.color.data_ptr())),
+              self.mpm.handle)
+
+    def add_prerender_passes(self) -> None:
+        """clearBuffer(massGrid), mass calculation, ray march (:345-356); read
+        the images after the handle's sync()."""
+        self.add_mass_calculation_dispatch(clear=True)
+        self.add_raymarch_dispatch()
+
+
 class GpuMpmBatch:
     """Many independent scenes advanced by the same launches: one handle, one
     scene table, particles concatenated in scene order.  Each scene keeps its

@@ -348,3 +348,24 @@ def parity_scene(kind="explicit", n_side=16, seed=10, res=32, with_collider=Fals
                       interaction=inter)
     params = reference_params(n_iter=n_iter, force_divisor=3.0, collider_margin=0.05)
     return SceneSpec(f"parity_{kind}", u, params, p, 1 if kind == "pbmpm" else 0, 1, mesh, res3)
+
+def camera_inv_view_proj(eye, target, width: int, height: int, up=(0, 0, 1), fovy_deg: float = 50.0,
+                         near: float = 0.05, far: float = 20.0) -> np.ndarray:
+    """viewProjInvMat of a look-at camera with a WebGPU perspective projection
+    (clip depth in [0, 1]), as the 16 column-major f32 the uniform block holds
+    at byte 112 (GpuUniformsBufferManager.write_view_proj_inv_mat)."""
+    eye, target, up = (np.asarray(v, np.float64) for v in (eye, target, up))
+    f = target - eye
+    f /= np.linalg.norm(f)
+    s = np.cross(f, up)
+    s /= np.linalg.norm(s)
+    u = np.cross(s, f)
+    view = np.eye(4)
+    view[0, :3], view[1, :3], view[2, :3] = s, u, -f
+    view[:3, 3] = -view[:3, :3] @ eye
+    t = 1.0 / np.tan(np.radians(fovy_deg) / 2)
+    proj = np.zeros((4, 4))
+    proj[0, 0], proj[1, 1] = t / (width / height), t
+    proj[2, 2], proj[2, 3] = far / (near - far), near * far / (near - far)
+    proj[3, 2] = -1.0
+    return np.linalg.inv(proj @ view).T.reshape(16).astype(np.float32)
