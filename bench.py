@@ -167,6 +167,7 @@ def cpu_reference(steps, warmup, sample_counts=(128, 32, 128)):
 # GPU arm
 # ----------------------------------------------------------------------
 def gpu_run(args, rank, world, local):
+    import numpy as np
     import torch
 
     torch.cuda.set_device(local)
@@ -310,6 +311,21 @@ def gpu_run(args, rank, world, local):
     splats["volumetric_raymarch"] = {"ms": round(ms_r, 4), "pixels": rw * rh,
                                      "covered": int((vol.output[..., 3] > 0).sum().item())}
     del vol, rpipe, mass_grid
+    # ---- collider BVH of the terrain (130,050 triangles): GPU build vs the host build
+    tv, tf = spec.mesh
+    tv_d = torch.from_numpy(np.ascontiguousarray(tv, np.float32)).cuda()
+    tf_d = torch.from_numpy(np.ascontiguousarray(tf, np.int32).reshape(-1)).cuda()
+    pkg.build_bvh_device(tv_d, tf_d, stream=stream.cuda_stream)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        pkg.build_bvh_device(tv_d, tf_d, stream=stream.cuda_stream)
+    gpu_bvh_ms = (time.perf_counter() - t0) / 3 * 1e3
+    t0 = time.perf_counter()
+    pkg.build_bvh(tv, tf)
+    host_bvh_ms = (time.perf_counter() - t0) * 1e3
+    splats["bvh_build"] = {"triangles": int(np.asarray(tf).size // 3), "gpu_ms": round(gpu_bvh_ms, 3),
+                           "host_ms": round(host_bvh_ms, 3)}
+    del tv_d, tf_d
     # ---- particle initialisation (scatterParticles) into a 1,280-triangle icosphere, 262,144 particles
     v_ico, f_ico = pkg.scenes.icosphere(3, 0.15, (0.5, 0.5, 0.5))
     mesh = pkg.GpuMeshBufferManager(vertices=v_ico, indices=f_ico)
@@ -327,7 +343,6 @@ def gpu_run(args, rank, world, local):
 
     # ---- end to end through the public API with host buffers
     host = torch.empty(n * 192, dtype=torch.uint8, pin_memory=True)
-    import numpy as np
     hv = host.numpy()
     hv[:] = np.frombuffer(spec.particles.tobytes(), np.uint8)
     e2e_steps = max(3, min(args.steps, 10))
@@ -558,6 +573,116 @@ def batched_leg(pkg, args, local, stream):
             "batched_vs_loop": loop_ms / ms, "unit": "particle-substeps/s"}
 
 
+def _agg_any(rec):
+    """_agg for 192-byte records or the f64 oracle's records."""
+    import numpy as np
+    if "Fe" in rec.dtype.names and rec["Fp"].ndim == 2:     # f64 oracle layout (9 entries per matrix)
+        m = rec["mass"].astype(np.float64)
+        v = rec["vel"].astype(np.float64)
+        com = (rec["pos"] * m[:, None]).sum(0) / m.sum()
+        mom = (v * m[:, None]).sum(0)
+        abs_mom = float((np.linalg.norm(v, axis=1) * m).sum())
+        jp = float(np.linalg.det(rec["Fp"].reshape(-1, 3, 3)).mean())
+        return com, mom, abs_mom, jp
+    return _agg(rec)
+
+
+def results_table(local):
+    """Rows of the results table: configs 0-2 on the GPU (CUDA-event
+    particle-substeps/s, P2G/G2P algorithmic GB/s), the f32 oracle on all host
+    cores over the same substeps (bit-exactness of the GPU result against it),
+    and the aggregate deviation of the GPU result from the f64 oracle."""
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # CPU restatement: the timed CPU baseline and the f64 error reference
+
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module(PKG)
+    lib = pkg.load()
+    threads = os.cpu_count() or 1
+    oracle.lib().orf_set_threads(threads)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    rows = []
+    cases = [("C0", pkg.scenes.c0_explicit_snow(), 100, 100),
+             ("C1", pkg.scenes.c1_pbmpm_spheres(), 100, 10),
+             ("C2 block", pkg.scenes.c2_large_pbmpm(counts=(128, 32, 128)), 60, 5)]
+    for name, spec, gpu_steps, cmp_steps in cases:
+        n = spec.particles.shape[0]
+        method = spec.method
+        # GPU throughput (state advanced by warm-up, graphs on)
+        buf, pipe = _pipeline(pkg, spec, 16, stream, local)
+        for _ in range(3):
+            pipe.step(method, 1)
+        buf.sync()
+        e0, e1 = _events(torch, stream)
+        e0.record(stream)
+        for _ in range(gpu_steps):
+            pipe.step(method, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        gpu_rate = n * gpu_steps / (e0.elapsed_time(e1) * 1e-3)
+        lib.mpm_enable_kernel_timing(buf.handle, 1)
+        for _ in range(5):
+            pipe.step(method, 1)
+        K = lib.mpm_kernel_count()
+        kms, kcnt = (C.c_float * K)(), (C.c_uint32 * K)()
+        lib.mpm_kernel_times(buf.handle, kms, kcnt, K)
+        lib.mpm_enable_kernel_timing(buf.handle, 0)
+        kn = pkg.kernel_names()
+        kt = {kn[i]: kms[i] / kcnt[i] for i in range(K) if kcnt[i]}
+        grid = buf.dense_grid(spec.res, apply_grid_update=False)
+        cells = int((grid[..., 0] != 0).sum())
+        del grid
+        buf.close()
+        if method == 0:
+            p2g = (n * (128 + 4) + cells * 16) / (kt["p2g_explicit"] * 1e-3) / 1e9
+            g2p = (cells * 16 + n * (4 + 88 + 144)) / (kt["g2p_explicit_integrate"] * 1e-3) / 1e9
+        else:
+            p2g = (n * (12 + 4 + 36 + 36 + 12 + 36 + 4) + cells * 16) / (kt["pbmpm_first"] * 1e-3) / 1e9
+            g2p = (cells * 16 + n * (4 + 88 + 144)) / (kt["g2p_pbmpm_integrate"] * 1e-3) / 1e9
+        # GPU result after cmp_steps substeps from the initial state
+        buf, pipe = _pipeline(pkg, spec, 16, stream, local)
+        for _ in range(cmp_steps):
+            pipe.step(method, 1)
+        status = buf.sync()
+        got = buf.read_particles()
+        buf.close()
+        # f32 oracle over the same substeps: timed CPU baseline and bit-exactness
+        o = oracle.Oracle(n, max_blocks=600000, hash_size=2000003)
+        if spec.mesh is not None:
+            o.set_collider(*spec.mesh)
+        p32 = spec.particles.copy()
+        t0 = time.perf_counter()
+        for _ in range(cmp_steps):
+            o.step(spec.uniforms.bytes(), spec.params, p32, method)
+        cpu_s = time.perf_counter() - t0
+        o.close()
+        def computed(r, f):   # matrices are three padded columns: compare the 3x3 part
+            a = r[f][:, :, :3] if f in ("Fe", "Fp", "D") else r[f]
+            return np.ascontiguousarray(a).view(np.uint32)
+        exact = all(np.array_equal(computed(got, f), computed(p32, f))
+                    for f in ("pos", "vel", "mass", "Fe", "Fp", "dxp", "D"))
+        # f64 oracle
+        o = oracle.Oracle(n, max_blocks=600000, hash_size=2000003, fp64=True)
+        if spec.mesh is not None:
+            o.set_collider(*spec.mesh)
+        p64 = oracle.to_fp64(spec.particles.copy())
+        for _ in range(cmp_steps):
+            o.step(spec.uniforms.bytes(), spec.params, p64, method)
+        o.close()
+        err = _agg_rel_err(_agg(got), _agg_any(p64))
+        rows.append({"config": name, "workload": spec.name, "particles": n, "method": "pbmpm" if method else "explicit",
+                     "gpu_value": gpu_rate, "gpu_steps": gpu_steps, "p2g_gbs": round(p2g, 1), "g2p_gbs": round(g2p, 1),
+                     "kernels_ms": {k: round(v, 4) for k, v in kt.items()}, "active_cells": cells,
+                     "cpu_value": n * cmp_steps / cpu_s, "cpu_threads": threads, "cpu_steps": cmp_steps,
+                     "bit_exact_vs_f32_oracle": bool(exact), "agg_rel_err_vs_f64": err, "device_status": status})
+        print(json.dumps(rows[-1]), flush=True)
+    return rows
+
+
 def mlp_case(local):
     """The network alone (the profiling case of its kernels): forward passes over
     1,048,576 random rows and one training epoch over 65,536 random pairs;
@@ -601,6 +726,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--mlp-case", action="store_true",
                     help="run only the learned-plasticity network on random rows (profiling case of its kernels)")
+    ap.add_argument("--results-table", action="store_true",
+                    help="measure configs 0-2 against the f32 and f64 oracles (one JSON line per config)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the learned-plasticity and batched-scene legs (they run at N = 1 only)")
     ap.add_argument("--counts", default="256,64,256",
@@ -610,6 +737,9 @@ def main():
     args.counts = tuple(int(v) for v in args.counts.split(","))
     if args.mlp_case:
         mlp_case(dist_env()[2])
+        return
+    if args.results_table:
+        results_table(dist_env()[2])
         return
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()

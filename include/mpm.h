@@ -129,6 +129,22 @@ int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* data, size_t 
  * nodes_out needs room for 2*n_tris+1 nodes; tri_order_out for n_tris. */
 int mpm_build_bvh(const float* vertices, uint32_t n_vertices, const uint32_t* indices,
                   uint32_t n_indices, void* nodes_out, uint32_t* tri_order_out, uint32_t* n_nodes_out);
+/* The same build on the GPU, node for node and bit for bit the tree of
+ * mpm_build_bvh (level-synchronous: per-node bounds by block reduction, the
+ * per-node stable centroid sort as one stable radix sort of (node, centroid)
+ * keys per level).  Device pointers; nodes_dev needs mpm_bvh_node_count(n_tris)
+ * nodes, tri_order_dev n_tris u32.  Enqueued on `stream` (a cudaStream_t, NULL
+ * for the default stream) and synchronised before returning; MPM_ERR_ARG if an
+ * index is >= n_vertices. */
+uint32_t mpm_bvh_node_count(uint32_t n_triangles);
+int mpm_build_bvh_device(const float* vertices_dev, uint32_t n_vertices, const uint32_t* indices_dev,
+                         uint32_t n_indices, void* nodes_dev, uint32_t* tri_order_dev, uint32_t* n_nodes_out,
+                         void* stream);
+/* A device-resident collider mesh installed without a host round trip: the
+ * BVH built on the GPU, the index buffer reordered into leaf order on the GPU,
+ * the collider buffer laid out as mpm_set_collider's (indices | vertices). */
+int mpm_set_collider_mesh_device(MpmHandle* h, uint32_t scene, const float* vertices_dev, uint32_t n_vertices,
+                                 const uint32_t* indices_dev, uint32_t n_indices);
 
 /* ---- the step (GpuMpmPipelineManager.ts:327-521) ------------------- */
 /* Enqueues n_substeps substeps of `method` on the handle's stream. */

@@ -6,10 +6,15 @@
  * 32-byte node packing (:183-202).  JavaScript numbers are f64 and
  * Array.prototype.sort is stable (ES2019), so bounds, extents and centroids
  * are computed in f64 and the per-node centroid sort is a stable merge sort.
+ * Math.min / Math.max order -0 below +0; js_min / js_max do the same.
  */
 #include "mpm_oracle.h"
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+static double js_min(double a, double b) { return (a < b || (a == b && signbit(a))) ? a : b; }
+static double js_max(double a, double b) { return (a > b || (a == b && !signbit(a))) ? a : b; }
 
 typedef struct {
     double mn[3], mx[3], ce[3];
@@ -50,8 +55,8 @@ static uint32_t rec(Build* b, uint32_t start, uint32_t end) {
     for (uint32_t i = start; i < end; i++) {
         const Tri* t = &b->tris[b->order[i]];
         for (int k = 0; k < 3; k++) {
-            if (t->mn[k] < mn[k]) mn[k] = t->mn[k];
-            if (t->mx[k] > mx[k]) mx[k] = t->mx[k];
+            mn[k] = js_min(mn[k], t->mn[k]);
+            mx[k] = js_max(mx[k], t->mx[k]);
         }
     }
     uint32_t* w = b->nodes + (size_t)node * 8;
@@ -93,8 +98,8 @@ uint32_t or_bvh_build(const float* v, uint32_t n_vertices, const uint32_t* idx, 
             for (int k = 0; k < 3; k++) p[j][k] = (double)v[(size_t)idx[i * 3 + j] * 3 + k];
         for (int k = 0; k < 3; k++) {
             double a = p[0][k], b = p[1][k], c = p[2][k];
-            double mn = a < b ? a : b; mn = mn < c ? mn : c;
-            double mx = a > b ? a : b; mx = mx > c ? mx : c;
+            double mn = js_min(js_min(a, b), c);
+            double mx = js_max(js_max(a, b), c);
             tris[i].mn[k] = mn;
             tris[i].mx[k] = mx;
             tris[i].ce[k] = ((a + b) + c) / 3.0;

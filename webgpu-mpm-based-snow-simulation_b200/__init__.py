@@ -11,13 +11,14 @@ from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams,
 from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
 from .pipeline import (GpuColliderBufferManager, GpuMeshBufferManager, GpuMpmBatch, GpuMpmBufferManager,
                        GpuMpmPipelineManager, GpuParticleInitializePipelineManager, GpuSimulationMethodType,
-                       GpuVolumetricBufferManager, GpuVolumetricRenderPipelineManager, build_bvh, kernel_names)
+                       GpuVolumetricBufferManager, GpuVolumetricRenderPipelineManager, build_bvh, build_bvh_device,
+                       kernel_names)
 
 __all__ = [
     "METHOD_EXPLICIT", "METHOD_PBMPM", "MpmConfig", "MpmError", "MpmParams", "default_params", "load",
     "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
     "GpuMpmBufferManager", "GpuMpmBatch", "GpuMpmPipelineManager", "GpuMeshBufferManager",
     "GpuParticleInitializePipelineManager", "GpuSimulationMethodType", "GpuVolumetricBufferManager",
-    "GpuVolumetricRenderPipelineManager", "build_bvh", "kernel_names",
+    "GpuVolumetricRenderPipelineManager", "build_bvh", "build_bvh_device", "kernel_names",
     "layout", "scenes", "learned", "batching",
 ]

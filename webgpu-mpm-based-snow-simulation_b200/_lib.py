@@ -131,6 +131,10 @@ SIGNATURES = {
     "mpm_scatter_particles": (C.c_int, [_H, C.c_void_p, C.c_uint32, C.c_uint32]),
     "mpm_grid_mass": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_int]),
     "mpm_mc_density": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]),
+    "mpm_bvh_node_count": (C.c_uint32, [C.c_uint32]),
+    "mpm_build_bvh_device": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_uint32), C.c_void_p]),
+    "mpm_set_collider_mesh_device": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
     "mpm_volumetric_raymarch": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                           C.c_void_p, C.c_void_p]),
     "mpm_mlp_init_params": (C.c_int, [C.c_uint32, C.c_void_p]),

@@ -7,8 +7,10 @@
 // triangles, nodes emitted in pre-order so a left child directly follows
 // its parent.  The reference computes in JavaScript f64 numbers and sorts
 // with the stable Array.prototype.sort; both are kept so node bounds and the
-// triangle order match it exactly.
+// triangle order match it exactly.  Math.min / Math.max order -0 below +0;
+// js_min / js_max do the same.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -16,6 +18,9 @@
 #include "../../include/mpm.h"
 
 namespace {
+
+double js_min(double a, double b) { return (a < b || (a == b && std::signbit(a))) ? a : b; }
+double js_max(double a, double b) { return (a > b || (a == b && !std::signbit(a))) ? a : b; }
 
 struct TriBox {
     double lo[3], hi[3], centroid[3];
@@ -38,8 +43,8 @@ struct Builder {
         for (uint32_t i = begin; i < end; i++) {
             const TriBox& t = tris[order[i]];
             for (int k = 0; k < 3; k++) {
-                lo[k] = std::min(lo[k], t.lo[k]);
-                hi[k] = std::max(hi[k], t.hi[k]);
+                lo[k] = js_min(lo[k], t.lo[k]);
+                hi[k] = js_max(hi[k], t.hi[k]);
             }
         }
         uint32_t* w = out + (size_t)id * 8;
@@ -91,8 +96,8 @@ extern "C" int mpm_build_bvh(const float* vertices, uint32_t n_vertices, const u
             for (int k = 0; k < 3; k++) v[j][k] = (double)vertices[(size_t)vi * 3 + k];
         }
         for (int k = 0; k < 3; k++) {
-            tris[i].lo[k] = std::min(std::min(v[0][k], v[1][k]), v[2][k]);
-            tris[i].hi[k] = std::max(std::max(v[0][k], v[1][k]), v[2][k]);
+            tris[i].lo[k] = js_min(js_min(v[0][k], v[1][k]), v[2][k]);
+            tris[i].hi[k] = js_max(js_max(v[0][k], v[1][k]), v[2][k]);
             tris[i].centroid[k] = ((v[0][k] + v[1][k]) + v[2][k]) / 3.0;
         }
     }

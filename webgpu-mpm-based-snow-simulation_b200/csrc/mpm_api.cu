@@ -43,6 +43,10 @@ struct ScatterArgs {
     float mmin[3], mmax[3];
 };
 cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t s);
+uint32_t bvh_node_count(uint32_t nt);
+int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t n_indices, void* nodes_dev,
+                     uint32_t* order_dev, cudaStream_t s, cudaError_t* cuda_err);
+cudaError_t reorder_indices(const uint32_t* idx, const uint32_t* order, uint32_t nt, uint32_t* out, cudaStream_t s);
 }  // namespace mpm
 
 using namespace mpm;
@@ -596,6 +600,44 @@ extern "C" int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* da
     s.dev.n_nodes = n_nodes;
     s.dev.c_nidx = num_indices;  // GpuMpmPipelineManager.ts:80 writes colliderNumIndices
     if (s.have_uniforms) std::memcpy(s.uni + 348, &num_indices, 4);
+    h->scenes_dirty = true;
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_collider_mesh_device(MpmHandle* h, uint32_t scene, const float* vertices_dev,
+                                            uint32_t n_vertices, const uint32_t* indices_dev, uint32_t n_indices) {
+    int r = check_scene(h, scene);
+    if (r) return r;
+    const uint32_t nt = n_indices / 3;
+    if (n_indices % 3) return fail(h, MPM_ERR_ARG, "n_indices %u is not a multiple of 3", n_indices);
+    if (nt && (!vertices_dev || !indices_dev)) return fail(h, MPM_ERR_ARG, "null mesh buffer");
+    cudaSetDevice(h->device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    SceneHost& s = h->scenes[scene];
+    if (s.col_data) { cudaFree(s.col_data); s.col_data = nullptr; }
+    if (s.bvh) { cudaFree(s.bvh); s.bvh = nullptr; }
+    const uint32_t n_nodes = bvh_node_count(nt);
+    const size_t words = (size_t)n_indices + (size_t)n_vertices * 3;
+    uint32_t* order = nullptr;
+    CK(h, cudaMalloc(&s.bvh, (size_t)n_nodes * MPM_BVH_NODE_BYTES));
+    if (words) CK(h, cudaMalloc(&s.col_data, words * 4));
+    if (nt) CK(h, cudaMalloc(&order, (size_t)nt * 4));
+    cudaError_t ce = cudaSuccess;
+    r = bvh_build_device(vertices_dev, n_vertices, indices_dev, n_indices, s.bvh, order, h->stream, &ce);
+    if (r == MPM_OK && nt) ce = reorder_indices(indices_dev, order, nt, s.col_data, h->stream);
+    if (r == MPM_OK && ce == cudaSuccess && n_vertices)
+        ce = cudaMemcpyAsync(s.col_data + n_indices, vertices_dev, (size_t)n_vertices * 12, cudaMemcpyDeviceToDevice,
+                             h->stream);
+    if (r == MPM_OK && ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+    if (order) cudaFree(order);
+    if (r == MPM_ERR_ARG) return fail(h, MPM_ERR_ARG, "mesh index >= n_vertices (%u)", n_vertices);
+    if (r != MPM_OK || ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "device BVH build: %s", cudaGetErrorString(ce));
+    s.dev.col_data = s.col_data;
+    s.dev.bvh = s.bvh;
+    s.dev.col_words = (uint32_t)words;
+    s.dev.n_nodes = n_nodes;
+    s.dev.c_nidx = n_indices;
+    if (s.have_uniforms) std::memcpy(s.uni + 348, &n_indices, 4);
     h->scenes_dirty = true;
     return MPM_OK;
 }

@@ -41,6 +41,29 @@ def build_bvh(vertices: np.ndarray, indices: np.ndarray):
     return nodes[: n.value].copy(), order[:nt].copy()
 
 
+def build_bvh_device(vertices, indices, stream: int | None = None):
+    """The same BVH built on the GPU from device-resident torch tensors
+    (vertices f32 [nv, 3], indices int32/uint32 [n_tris * 3]).  Returns (nodes
+    int32 CUDA tensor [n, 8] holding the 32-byte nodes, triangle order)."""
+    import torch
+
+    v = vertices.contiguous().view(-1)
+    idx = indices.contiguous().view(-1)
+    if v.dtype != torch.float32 or idx.dtype not in (torch.int32, torch.uint32) or not v.is_cuda or not idx.is_cuda:
+        raise TypeError("vertices: float32 CUDA tensor, indices: int32 CUDA tensor")
+    nt = idx.numel() // 3
+    lib = load()
+    n_nodes = lib.mpm_bvh_node_count(nt)
+    nodes = torch.empty((n_nodes, 8), dtype=torch.int32, device=v.device)
+    order = torch.empty(max(nt, 1), dtype=torch.int32, device=v.device)
+    n = C.c_uint32(0)
+    s = torch.cuda.current_stream(v.device).cuda_stream if stream is None else stream
+    check(lib.mpm_build_bvh_device(C.c_void_p(v.data_ptr()), v.numel() // 3, C.c_void_p(idx.data_ptr()), idx.numel(),
+                                   C.c_void_p(nodes.data_ptr()), C.c_void_p(order.data_ptr()), C.byref(n),
+                                   C.c_void_p(s)))
+    return nodes[: n.value], order[:nt]
+
+
 class GpuColliderBufferManager:
     """Packs a collider mesh the way the reference does: one u32 buffer
     [indices in BVH leaf order | vertices f32x3 | normals | uvs | material
@@ -196,6 +219,22 @@ class GpuMpmPipelineManager:
                                              collider_manager.num_indices, nodes.ctypes.data, nodes.shape[0]),
                   self.mpm.handle)
         self._last_uniforms = None
+        self.push_uniforms()
+
+    def set_collider_mesh_device(self, vertices, indices) -> None:
+        """Installs a device-resident collider mesh (torch CUDA tensors): BVH
+        built and indices reordered on the GPU (mpm_set_collider_mesh_device).
+        Collider bounds and transform stay the uniform writer's business, as
+        with GpuColliderBufferManager."""
+        import torch
+
+        torch.cuda.current_stream().synchronize()
+        v = vertices.contiguous().view(-1)
+        idx = indices.contiguous().view(-1)
+        self.uniforms.write_collider_num_indices(idx.numel())
+        check(self._lib.mpm_set_collider_mesh_device(self.mpm.handle, self.scene, C.c_void_p(v.data_ptr()),
+                                                     v.numel() // 3, C.c_void_p(idx.data_ptr()), idx.numel()),
+              self.mpm.handle)
         self.push_uniforms()
 
     def push_uniforms(self) -> None:
