@@ -273,7 +273,14 @@ def gpu_run(args, rank, world, local):
     torch.cuda.synchronize()
     ex_rate = n * ex_steps / (e0.elapsed_time(e1) * 1e-3)
 
-    # ---- renderer splats of the final state (calculateGridMass.wgsl, mcDensity.cs.wgsl)
+    # ---- renderer passes of the final state.  The step's fixed-point scale
+    # (2^45, sized for the momentum sums) would wrap the renderers' u32 mass
+    # sums, so they run with a scale of 2^20, restored afterwards.
+    u_bytes = spec.uniforms.bytes()
+    step_scale = float(np.frombuffer(bytes(u_bytes[4:8]), "<f4")[0])
+    spec.uniforms.write_fixed_point_scale(2.0 ** 20)
+    pipe.push_uniforms()
+    # ---- renderer splats (calculateGridMass.wgsl, mcDensity.cs.wgsl)
     rx, ry, rz = spec.res
     mass_grid = torch.zeros((rz, ry, rx), dtype=torch.int32, device="cuda")
     dens_grid = torch.zeros((rz // 2, ry // 2, rx // 2), dtype=torch.int32, device="cuda")
@@ -311,6 +318,23 @@ def gpu_run(args, rank, world, local):
     splats["volumetric_raymarch"] = {"ms": round(ms_r, 4), "pixels": rw * rh,
                                      "covered": int((vol.output[..., 3] > 0).sum().item())}
     del vol, rpipe, mass_grid
+    # ---- marching cubes of the final state: 256^3 MC grid over an 8^3 density
+    # grid (cells of 1/8: the slab's mass per cell, up to ~0.57, crosses the
+    # isovalue 0.15; at fine density grids it stays below it, the mesh is empty)
+    mcb = pkg.GpuMarchingCubesBufferManager(grid_resolution=(16, 16, 16), mc_grid_resolution=(256, 256, 256),
+                                            device=local, max_vertices=6_000_000)
+    mcp = pkg.GpuMarchingCubesRenderPipelineManager(mpm_manager=buf, mc_manager=mcb)
+    mcp.add_mesh_generation_pass()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        mcp.add_mesh_generation_pass()
+    mc_ms = (time.perf_counter() - t0) / 3 * 1e3
+    splats["marching_cubes"] = {"ms_wall": round(mc_ms, 3), "mc_res": list(mcb.mc_grid_resolution),
+                                "vertices": mcb.vertices_generated}
+    del mcp, mcb
+    spec.uniforms.write_fixed_point_scale(step_scale)
+    pipe.push_uniforms()
     # ---- collider BVH of the terrain (130,050 triangles): GPU build vs the host build
     tv, tf = spec.mesh
     tv_d = torch.from_numpy(np.ascontiguousarray(tv, np.float32)).cuda()

@@ -213,6 +213,25 @@ int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32_t n_vertic
 int mpm_grid_mass(MpmHandle* h, uint32_t scene, uint32_t* out_dev, int accumulate);
 int mpm_mc_density(MpmHandle* h, uint32_t scene, const uint32_t* density_res, uint32_t* out_dev, int accumulate);
 
+/* ---- marching cubes --------------------------------------------------- */
+/* The mesh-generation passes of GpuMarchingCubesRenderPipelineManager
+ * (src/lib/gpu/marchingCubes/GpuMarchingCubesRenderPipelineManager.ts:587-633:
+ * mcListBlocks, mcVertexDensity, mcGenerate, mcClampArgs) over a density grid
+ * made by mpm_mc_density: vertices_dev receives 6 f32 per vertex (position,
+ * normal), 3 vertices per triangle, in a deterministic order (active 8^3
+ * blocks ascending, cells in block order, triangles in table order); at most
+ * max_vertices are written.  *vertex_count_out = min(generated, max_vertices)
+ * (the clamped draw count), *vertices_generated_out (optional) = generated.
+ * The triangulation table is this library's (mpm_mc_tables): the iso-contour
+ * traced around the cube with inside corners kept apart on ambiguous faces,
+ * the reference's vertex and edge numbering.  Synchronises the stream. */
+int mpm_marching_cubes(MpmHandle* h, uint32_t scene, const uint32_t* density_dev, const uint32_t* density_res,
+                       const uint32_t* mc_res, float* vertices_dev, uint32_t max_vertices,
+                       uint32_t* vertex_count_out, uint32_t* vertices_generated_out);
+/* tri_out 256 x 16 edge indices (-1 padded), count_out 256 triangle counts,
+ * edge_vertices_out 12 x 2 cube vertex ids; any may be NULL. */
+int mpm_mc_tables(int8_t* tri_out, uint8_t* count_out, uint8_t* edge_vertices_out);
+
 /* ---- volumetric ray march ------------------------------------------- */
 /* doVolumetricRaymarch (src/lib/gpu/volumetric/volumetricRaymarch.cs.wgsl:118-226,
  * dispatched by GpuVolumetricRenderPipelineManager.addRaymarchDispatch,

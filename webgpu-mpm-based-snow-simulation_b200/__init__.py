@@ -9,7 +9,8 @@ generators.
 from . import _lib, batching, layout, learned, scenes
 from ._lib import METHOD_EXPLICIT, METHOD_PBMPM, MpmConfig, MpmError, MpmParams, default_params, load
 from .layout import PARTICLE_DTYPE, GpuUniformsBufferManager, new_particles
-from .pipeline import (GpuColliderBufferManager, GpuMeshBufferManager, GpuMpmBatch, GpuMpmBufferManager,
+from .pipeline import (GpuColliderBufferManager, GpuMarchingCubesBufferManager,
+                       GpuMarchingCubesRenderPipelineManager, GpuMeshBufferManager, GpuMpmBatch, GpuMpmBufferManager,
                        GpuMpmPipelineManager, GpuParticleInitializePipelineManager, GpuSimulationMethodType,
                        GpuVolumetricBufferManager, GpuVolumetricRenderPipelineManager, build_bvh, build_bvh_device,
                        kernel_names)
@@ -19,6 +20,7 @@ __all__ = [
     "PARTICLE_DTYPE", "GpuUniformsBufferManager", "new_particles", "GpuColliderBufferManager",
     "GpuMpmBufferManager", "GpuMpmBatch", "GpuMpmPipelineManager", "GpuMeshBufferManager",
     "GpuParticleInitializePipelineManager", "GpuSimulationMethodType", "GpuVolumetricBufferManager",
-    "GpuVolumetricRenderPipelineManager", "build_bvh", "build_bvh_device", "kernel_names",
+    "GpuVolumetricRenderPipelineManager", "GpuMarchingCubesBufferManager", "GpuMarchingCubesRenderPipelineManager",
+    "build_bvh", "build_bvh_device", "kernel_names",
     "layout", "scenes", "learned", "batching",
 ]

@@ -131,6 +131,9 @@ SIGNATURES = {
     "mpm_scatter_particles": (C.c_int, [_H, C.c_void_p, C.c_uint32, C.c_uint32]),
     "mpm_grid_mass": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_int]),
     "mpm_mc_density": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]),
+    "mpm_marching_cubes": (C.c_int, [_H, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                     C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "mpm_mc_tables": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mpm_bvh_node_count": (C.c_uint32, [C.c_uint32]),
     "mpm_build_bvh_device": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                        C.POINTER(C.c_uint32), C.c_void_p]),

@@ -47,6 +47,9 @@ uint32_t bvh_node_count(uint32_t nt);
 int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t n_indices, void* nodes_dev,
                      uint32_t* order_dev, cudaStream_t s, cudaError_t* cuda_err);
 cudaError_t reorder_indices(const uint32_t* idx, const uint32_t* order, uint32_t nt, uint32_t* out, cudaStream_t s);
+int mc_run(const uint32_t* density, const uint32_t* dres, const uint32_t* mres, const float* gmin, const float* gmax,
+           float scale, float* out, uint32_t max_vertices, uint32_t* vertices_total, int n_sms, cudaStream_t s,
+           cudaError_t* err);
 }  // namespace mpm
 
 using namespace mpm;
@@ -1125,6 +1128,34 @@ extern "C" int mpm_volumetric_raymarch(MpmHandle* h, uint32_t scene, const uint3
     a.depth = depth_dev;
     a.color = color_dev;
     CK(h, launch_raymarch(a, h->stream));
+    return MPM_OK;
+}
+
+// Marching cubes (mcListBlocks, mcVertexDensity, mcGenerate) over a density
+// grid of the mcDensity splat; grid bounds and fixed-point scale of the scene.
+extern "C" int mpm_marching_cubes(MpmHandle* h, uint32_t scene, const uint32_t* density_dev,
+                                  const uint32_t* density_res, const uint32_t* mc_res, float* vertices_dev,
+                                  uint32_t max_vertices, uint32_t* vertex_count_out, uint32_t* vertices_generated_out) {
+    if (!h) return MPM_ERR_ARG;
+    int r = check_scene(h, scene);
+    if (r) return r;
+    if (scene >= h->n_scenes) return fail(h, MPM_ERR_ARG, "scene %u >= scene count", scene);
+    if (!density_dev || !density_res || !mc_res || !vertex_count_out || (max_vertices && !vertices_dev))
+        return fail(h, MPM_ERR_ARG, "null argument");
+    for (int k = 0; k < 3; k++)
+        if (density_res[k] == 0 || mc_res[k] == 0 || mc_res[k] > 4096 || density_res[k] > 4096)
+            return fail(h, MPM_ERR_ARG, "grid resolutions must be in 1..4096");
+    cudaSetDevice(h->device);
+    r = upload_scenes(h);
+    if (r) return r;
+    const SceneDev& d = h->scenes[scene].dev;
+    uint32_t total = 0;
+    cudaError_t ce = cudaSuccess;
+    if (mc_run(density_dev, density_res, mc_res, d.gmin, d.gmax, d.scale, vertices_dev, max_vertices, &total, h->n_sms,
+               h->stream, &ce))
+        return fail(h, MPM_ERR_CUDA, "marching cubes: %s", cudaGetErrorString(ce));
+    *vertex_count_out = total < max_vertices ? total : max_vertices;   // mcClampArgs
+    if (vertices_generated_out) *vertices_generated_out = total;
     return MPM_OK;
 }
 

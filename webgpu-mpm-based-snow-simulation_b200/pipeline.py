@@ -372,6 +372,79 @@ class GpuVolumetricRenderPipelineManager:
         self.add_raymarch_dispatch()
 
 
+N_MAX_MC_VERTICES = 10_500_000   # GpuMarchingCubesBufferManager.ts:1-2 (3.5 M triangles)
+
+
+class GpuMarchingCubesBufferManager:
+    """Device buffers of the marching-cubes renderer (GpuMarchingCubesBufferManager.ts),
+    headless: the u32 density grid (half the simulation resolution by default),
+    the vertex buffer (6 f32 per vertex: position, normal) and the vertex
+    count the draw would use."""
+
+    def __init__(self, *, grid_resolution, mc_grid_resolution=None, device: int = 0,
+                 max_vertices: int = N_MAX_MC_VERTICES):
+        import torch
+
+        gx, gy, gz = (int(r) for r in grid_resolution)
+        self.density_grid_resolution = (gx // 2, gy // 2, gz // 2)
+        self.mc_grid_resolution = tuple(int(r) for r in mc_grid_resolution) if mc_grid_resolution is not None \
+            else (gx // 2, gy // 2, gz // 2)
+        self.device = device
+        dx, dy, dz = self.density_grid_resolution
+        dev = f"cuda:{device}"
+        self.density_grid = torch.zeros((dz, dy, dx), dtype=torch.int32, device=dev)
+        self.max_vertices = int(max_vertices)
+        self.vertices = torch.zeros((self.max_vertices, 6), dtype=torch.float32, device=dev)
+        self.vertex_count = 0
+        self.vertices_generated = 0
+
+
+class GpuMarchingCubesRenderPipelineManager:
+    """addMeshGenerationPass (GpuMarchingCubesRenderPipelineManager.ts:587-633):
+    clear + calculateDensity, then listBlocks, computeVertexDensity,
+    generateMesh and the draw-count clamp.  The mesh draw and shading passes
+    are graphics work with no headless counterpart: the vertex buffer is the
+    result."""
+
+    def __init__(self, *, mpm_manager: GpuMpmBufferManager, mc_manager: GpuMarchingCubesBufferManager,
+                 scene: int = 0):
+        self.mpm = mpm_manager
+        self.mc = mc_manager
+        self.scene = scene
+        self._lib = load()
+
+    def add_density_dispatch(self) -> None:
+        m = self.mc
+        res = (C.c_uint32 * 3)(*m.density_grid_resolution)
+        check(self._lib.mpm_mc_density(self.mpm.handle, self.scene, res, C.c_void_p(m.density_grid.data_ptr()), 0),
+              self.mpm.handle)
+
+    def add_mesh_dispatches(self) -> int:
+        m = self.mc
+        dres = (C.c_uint32 * 3)(*m.density_grid_resolution)
+        mres = (C.c_uint32 * 3)(*m.mc_grid_resolution)
+        cnt, gen = C.c_uint32(0), C.c_uint32(0)
+        check(self._lib.mpm_marching_cubes(self.mpm.handle, self.scene, C.c_void_p(m.density_grid.data_ptr()), dres,
+                                           mres, C.c_void_p(m.vertices.data_ptr()), m.max_vertices, C.byref(cnt),
+                                           C.byref(gen)), self.mpm.handle)
+        m.vertex_count, m.vertices_generated = cnt.value, gen.value
+        return cnt.value
+
+    def add_mesh_generation_pass(self) -> int:
+        """Density splat and mesh generation; returns the vertex count."""
+        self.add_density_dispatch()
+        return self.add_mesh_dispatches()
+
+
+def mc_tables():
+    """(triangle table int8 [256, 16], counts uint8 [256], edge endpoints uint8 [12, 2])."""
+    tri = np.zeros((256, 16), np.int8)
+    cnt = np.zeros(256, np.uint8)
+    ev = np.zeros((12, 2), np.uint8)
+    check(load().mpm_mc_tables(tri.ctypes.data, cnt.ctypes.data, ev.ctypes.data))
+    return tri, cnt, ev
+
+
 class GpuMpmBatch:
     """Many independent scenes advanced by the same launches: one handle, one
     scene table, particles concatenated in scene order.  Each scene keeps its
