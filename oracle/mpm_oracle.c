@@ -77,8 +77,8 @@ static inline double u2d(uint64_t u) { double d; memcpy(&d, &u, 8); return d; }
 static inline double pow2i(int k) { return u2d((uint64_t)(k + 1023) << 52); }
 
 /* exp(x) in f64: Cody-Waite reduction x = k*ln2 + r, |r| <= ln2/2, then the
- * Taylor series of e^r to degree 13 by Horner (truncation error < 1e-17
- * relative), then scaling by 2^k in two exact steps. */
+ * Taylor series of e^r to degree 13 by Horner with fused multiply-adds
+ * (truncation error < 1e-17 relative), then scaling by 2^k in two exact steps. */
 double or_exp64(double x) {
     if (x != x) return x;
     if (x > 709.782712893384) return INFINITY;
@@ -90,25 +90,26 @@ double or_exp64(double x) {
     int k = (int)kf;
     double r = (x - kf * LN2_HI) - kf * LN2_LO;
     double p = 1.0 / 6227020800.0;               /* 1/13! */
-    p = p * r + 1.0 / 479001600.0;               /* 1/12! */
-    p = p * r + 1.0 / 39916800.0;
-    p = p * r + 1.0 / 3628800.0;
-    p = p * r + 1.0 / 362880.0;
-    p = p * r + 1.0 / 40320.0;
-    p = p * r + 1.0 / 5040.0;
-    p = p * r + 1.0 / 720.0;
-    p = p * r + 1.0 / 120.0;
-    p = p * r + 1.0 / 24.0;
-    p = p * r + 1.0 / 6.0;
-    p = p * r + 0.5;
-    p = p * r + 1.0;
-    p = p * r + 1.0;
+    p = fma(p, r, 1.0 / 479001600.0);               /* 1/12! */
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
     int k1 = k / 2, k2 = k - k1;
     return (p * pow2i(k1)) * pow2i(k2);
 }
 
 /* log(x) in f64: x = m * 2^e with m in [sqrt(1/2), sqrt(2)), then
- * log(m) = 2*atanh(s), s = (m-1)/(m+1), by its odd power series to s^23. */
+ * log(m) = 2*atanh(s), s = (m-1)/(m+1), by its odd power series to s^23
+ * (Horner in s^2 with fused multiply-adds). */
 double or_log64(double x) {
     if (x != x || x < 0.0) return NAN;
     if (x == 0.0) return -INFINITY;
@@ -126,17 +127,17 @@ double or_log64(double x) {
     double s = (m - 1.0) / (m + 1.0);
     double s2 = s * s;
     double q = 1.0 / 23.0;
-    q = q * s2 + 1.0 / 21.0;
-    q = q * s2 + 1.0 / 19.0;
-    q = q * s2 + 1.0 / 17.0;
-    q = q * s2 + 1.0 / 15.0;
-    q = q * s2 + 1.0 / 13.0;
-    q = q * s2 + 1.0 / 11.0;
-    q = q * s2 + 1.0 / 9.0;
-    q = q * s2 + 1.0 / 7.0;
-    q = q * s2 + 1.0 / 5.0;
-    q = q * s2 + 1.0 / 3.0;
-    q = q * s2 + 1.0;
+    q = fma(q, s2, 1.0 / 21.0);
+    q = fma(q, s2, 1.0 / 19.0);
+    q = fma(q, s2, 1.0 / 17.0);
+    q = fma(q, s2, 1.0 / 15.0);
+    q = fma(q, s2, 1.0 / 13.0);
+    q = fma(q, s2, 1.0 / 11.0);
+    q = fma(q, s2, 1.0 / 9.0);
+    q = fma(q, s2, 1.0 / 7.0);
+    q = fma(q, s2, 1.0 / 5.0);
+    q = fma(q, s2, 1.0 / 3.0);
+    q = fma(q, s2, 1.0);
     const double LN2 = 6.93147180559945309417e-01;
     return (double)e * LN2 + 2.0 * s * q;
 }

@@ -332,7 +332,7 @@ int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t 
                  o_perm = carve((size_t)nt * 4 * 2), o_klo = carve((size_t)nt * 8 * 2), o_khi = carve((size_t)nt * 4 * 2),
                  o_cnt = carve((size_t)256 * nb * 4), o_plan = carve(by_level.size() * sizeof(NodePlan)),
                  o_err = carve(4);
-    cudaError_t e = cudaMalloc(&ws, off);
+    cudaError_t e = cudaMallocAsync(&ws, off, s);
     if (e != cudaSuccess) {
         *cuda_err = e;
         return MPM_ERR_CUDA;
@@ -372,8 +372,8 @@ int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t 
     if (e == cudaSuccess) e = cudaMemcpyAsync(order_dev, perm[cur], (size_t)nt * 4, cudaMemcpyDeviceToDevice, s);
     int herr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(ws, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(ws);
     *cuda_err = e;
     if (e != cudaSuccess) return MPM_ERR_CUDA;
     return herr ? MPM_ERR_ARG : MPM_OK;

@@ -1068,6 +1068,42 @@ __device__ __forceinline__ void g2p_gather(const TileCtx<E>& T, const float4* ve
             for (int a = 0; a < 3; a++) dwv[k][a] = dwk(k, sc.f[a]);
     }
     const float4* row = vel + (l0[2] * H + l0[1]) * H + l0[0];
+    if (PB) {
+        // the same sums in paired form: (nv0, nv1), (G[3c], G[3c+1]) per
+        // column c, (G[2], G[5]); nv2 and G[8] scalar
+        float2 nv01 = make_float2(0.f, 0.f), g01[3], g25 = make_float2(0.f, 0.f);
+        float nv2 = 0.f, g8 = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) g01[c] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int oz = 0; oz < 3; oz++)
+#pragma unroll
+            for (int oy = 0; oy < 3; oy++) {
+                float wxy[3];
+#pragma unroll
+                for (int ox = 0; ox < 3; ox++) wxy[ox] = fm(sc.w[ox][0], sc.w[oy][1]);
+#pragma unroll
+                for (int ox = 0; ox < 3; ox++) {
+                    float4 c4 = row[(oz * H + oy) * H + ox];
+                    const float wgt = fm(wxy[ox], sc.w[oz][2]);
+                    const float2 w2 = dup2(wgt), cv01 = make_float2(c4.x, c4.y);
+                    nv01 = ff2(w2, cv01, nv01);
+                    nv2 = ff(wgt, c4.z, nv2);
+                    const float2 wv01 = fm2(w2, cv01);
+                    const float wv2 = fm(wgt, c4.z);
+                    const float dist[3] = {offs[0][ox], offs[1][oy], offs[2][oz]};
+#pragma unroll
+                    for (int c = 0; c < 3; c++) g01[c] = ff2(wv01, dup2(dist[c]), g01[c]);
+                    g25 = ff2(dup2(wv2), make_float2(dist[0], dist[1]), g25);
+                    g8 = ff(wv2, dist[2], g8);
+                }
+            }
+        nv[0] = nv01.x; nv[1] = nv01.y; nv[2] = nv2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) { G[3 * c] = g01[c].x; G[3 * c + 1] = g01[c].y; }
+        G[2] = g25.x; G[5] = g25.y; G[8] = g8;
+        return;
+    }
 #pragma unroll
     for (int oz = 0; oz < 3; oz++)
 #pragma unroll
@@ -1180,6 +1216,38 @@ __device__ __forceinline__ void p2g_pbmpm_particle(const SceneDev& S, const Tile
 #pragma unroll
     for (int k = 0; k < 3; k++) fon[k] = iact || S.gdiv[k] != 0.0f;
     uint32_t* base = acc + (l0[2] * H + l0[1]) * H + l0[0];
+    if (FOLD && !iact) {
+        // components 0 and 1 in paired form, component 2 scalar; same
+        // per-component operations as the general loop below
+        const float2 D01 = make_float2(D[0], D[1]), D34 = make_float2(D[3], D[4]), D67 = make_float2(D[6], D[7]);
+        const float2 dxp01 = make_float2(dxp[0], dxp[1]), rdts2 = dup2(S.rdts);
+#pragma unroll
+        for (int oy = 0; oy < 3; oy++)
+#pragma unroll
+            for (int ox = 0; ox < 3; ox++) {
+                const float2 pxy01 = ff2(D34, dup2(off[1][oy]), fm2(D01, dup2(off[0][ox])));
+                const float pxy2 = ff(D[5], off[1][oy], fm(D[2], off[0][ox]));
+                const float wxy = fm(sc.w[ox][0], sc.w[oy][1]);
+#pragma unroll
+                for (int oz = 0; oz < 3; oz++) {
+                    const float wgt = fm(wxy, sc.w[oz][2]);
+                    const float wm = fm(wgt, mass);
+                    const float2 aff01 = ff2(D67, dup2(off[2][oz]), pxy01);
+                    const float aff2 = ff(D[8], off[2][oz], pxy2);
+                    const float2 x01 = fm2(fm2(dup2(wm), fa2(dxp01, aff01)), rdts2);
+                    uint32_t v[3] = {(uint32_t)f2i(x01.x), (uint32_t)f2i(x01.y),
+                                     (uint32_t)f2i(fm(fm(wm, fa(dxp[2], aff2)), S.rdts))};
+#pragma unroll
+                    for (int k = 0; k < 3; k++)
+                        if (fon[k]) v[k] += (uint32_t)enc_dt<FOLD>(S, fm(S.gdiv[k], wm));
+                    uint32_t* cell = base + (oz * H + oy) * H + ox;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) atomicAdd(cell + (k + (WITH_MASS ? 1 : 0)) * NC, v[k]);
+                    if (WITH_MASS) atomicAdd(cell, (uint32_t)f2i(fm(wm, S.scale)));
+                }
+            }
+        return;
+    }
 #pragma unroll
     for (int oy = 0; oy < 3; oy++)
 #pragma unroll(FOLD ? 3 : 1)

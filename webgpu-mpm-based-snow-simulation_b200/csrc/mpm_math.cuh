@@ -69,11 +69,12 @@ __host__ __device__ __forceinline__ uint32_t hash4(uint32_t x, uint32_t y, uint3
 }
 
 // exp(x) in f64: Cody-Waite reduction x = k ln2 + r, then the degree-13
-// Taylor polynomial of e^r (Horner), then exact scaling by 2^k.
+// Taylor polynomial of e^r (Horner, one fused multiply-add per step), then
+// exact scaling by 2^k.
 __device__ __forceinline__ double pow2i(int k) {
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
-static __device__ __noinline__ double exp64(double x) {
+static __device__ __forceinline__ double exp64(double x) {
     if (x != x) return x;
     if (x > 709.782712893384) return __longlong_as_double(0x7ff0000000000000ll);
     if (x < -745.2) return 0.0;
@@ -84,26 +85,27 @@ static __device__ __noinline__ double exp64(double x) {
     int k = (int)kf;
     double r = __dsub_rn(__dsub_rn(x, __dmul_rn(kf, LN2_HI)), __dmul_rn(kf, LN2_LO));
     double p = 1.0 / 6227020800.0;
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 479001600.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 39916800.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 3628800.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 362880.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 40320.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 5040.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 720.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 120.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 24.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0 / 6.0);
-    p = __dadd_rn(__dmul_rn(p, r), 0.5);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0);
+    p = __fma_rn(p, r, 1.0 / 479001600.0);
+    p = __fma_rn(p, r, 1.0 / 39916800.0);
+    p = __fma_rn(p, r, 1.0 / 3628800.0);
+    p = __fma_rn(p, r, 1.0 / 362880.0);
+    p = __fma_rn(p, r, 1.0 / 40320.0);
+    p = __fma_rn(p, r, 1.0 / 5040.0);
+    p = __fma_rn(p, r, 1.0 / 720.0);
+    p = __fma_rn(p, r, 1.0 / 120.0);
+    p = __fma_rn(p, r, 1.0 / 24.0);
+    p = __fma_rn(p, r, 1.0 / 6.0);
+    p = __fma_rn(p, r, 0.5);
+    p = __fma_rn(p, r, 1.0);
+    p = __fma_rn(p, r, 1.0);
     int k1 = k / 2, k2 = k - k1;
     return __dmul_rn(__dmul_rn(p, pow2i(k1)), pow2i(k2));
 }
 
 // log(x) in f64: x = m 2^e, m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s),
-// s = (m-1)/(m+1), odd power series to s^23.
-static __device__ __noinline__ double log64(double x) {
+// s = (m-1)/(m+1), odd power series to s^23 (Horner in s^2 with fused
+// multiply-adds).
+static __device__ __forceinline__ double log64(double x) {
     if (x != x || x < 0.0) return __longlong_as_double(0x7ff8000000000000ll);
     if (x == 0.0) return __longlong_as_double((long long)0xfff0000000000000ull);
     if (x == __longlong_as_double(0x7ff0000000000000ll)) return x;
@@ -120,17 +122,17 @@ static __device__ __noinline__ double log64(double x) {
     double s = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
     double s2 = __dmul_rn(s, s);
     double q = 1.0 / 23.0;
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 21.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 19.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 17.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 15.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 13.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 11.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 9.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 7.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 5.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0 / 3.0);
-    q = __dadd_rn(__dmul_rn(q, s2), 1.0);
+    q = __fma_rn(q, s2, 1.0 / 21.0);
+    q = __fma_rn(q, s2, 1.0 / 19.0);
+    q = __fma_rn(q, s2, 1.0 / 17.0);
+    q = __fma_rn(q, s2, 1.0 / 15.0);
+    q = __fma_rn(q, s2, 1.0 / 13.0);
+    q = __fma_rn(q, s2, 1.0 / 11.0);
+    q = __fma_rn(q, s2, 1.0 / 9.0);
+    q = __fma_rn(q, s2, 1.0 / 7.0);
+    q = __fma_rn(q, s2, 1.0 / 5.0);
+    q = __fma_rn(q, s2, 1.0 / 3.0);
+    q = __fma_rn(q, s2, 1.0);
     const double LN2 = 6.93147180559945309417e-01;
     return __dadd_rn(__dmul_rn((double)e, LN2), __dmul_rn(__dmul_rn(2.0, s), q));
 }
@@ -148,6 +150,13 @@ __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); 
 __device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
 
 __device__ __forceinline__ float ff(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// Paired f32 operations (one FFMA2 / FMUL2 / FADD2 instruction on sm_100 for
+// two lanes); each component rounds exactly as the scalar op above.
+__device__ __forceinline__ float2 ff2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 fm2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fa2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 
 __device__ __forceinline__ float dot3(const float* a, const float* b) {
     return ff(a[2], b[2], ff(a[1], b[1], fm(a[0], b[0])));
@@ -183,7 +192,7 @@ __device__ __forceinline__ void inv3(const float* m, float* o) {
     float a6 = ff(m[3], m[7], -fm(m[4], m[6]));
     float a7 = ff(m[1], m[6], -fm(m[0], m[7]));
     float a8 = ff(m[0], m[4], -fm(m[1], m[3]));
-    float s = fd(1.0f, det);
+    float s = __frcp_rn(det);   // RN(1/det), the IEEE quotient 1/det
     o[0] = fm(a0, s); o[1] = fm(a1, s); o[2] = fm(a2, s);
     o[3] = fm(a3, s); o[4] = fm(a4, s); o[5] = fm(a5, s);
     o[6] = fm(a6, s); o[7] = fm(a7, s); o[8] = fm(a8, s);
