@@ -226,14 +226,26 @@ __device__ __forceinline__ void pbmpm_constraints(const SceneDev& S, const float
     float vs = powf_m(fabsf(tv), S.vexp);
     float ob = fs(1.0f, S.blend);
     float tb[9], Dc[9];
+    // tb = blend (R vs) + (1 - blend) R, D += relax (Dc - I - D), in pairs
+    const float2 vs2 = dup2(vs), ob2 = dup2(ob), bl2 = dup2(S.blend), rx2 = dup2(relax);
 #pragma unroll
-    for (int i = 0; i < 9; i++) tb[i] = ff(S.blend, fm(Rt[i], vs), fm(ob, Rt[i]));
+    for (int i = 0; i < 8; i += 2) {
+        const float2 r = make_float2(Rt[i], Rt[i + 1]);
+        const float2 v = ff2(bl2, fm2(r, vs2), fm2(ob2, r));
+        tb[i] = v.x;
+        tb[i + 1] = v.y;
+    }
+    tb[8] = ff(S.blend, fm(Rt[8], vs), fm(ob, Rt[8]));
     mul3(tb, Fei, Dc);
 #pragma unroll
-    for (int i = 0; i < 9; i++) {
-        float dci = fs(Dc[i], (i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f);
-        D[i] = ff(relax, fs(dci, D[i]), D[i]);
+    for (int i = 0; i < 8; i += 2) {
+        const float2 id = make_float2((i == 0 || i == 4) ? 1.0f : 0.0f, (i + 1 == 4) ? 1.0f : 0.0f);
+        const float2 d = make_float2(D[i], D[i + 1]);
+        const float2 v = ff2(rx2, fa2(fa2(make_float2(Dc[i], Dc[i + 1]), neg2(id)), neg2(d)), d);
+        D[i] = v.x;
+        D[i + 1] = v.y;
     }
+    D[8] = ff(relax, fs(fs(Dc[8], 1.0f), D[8]), D[8]);
 }
 
 // applyPlasticity (plasticityOps.wgsl:7-48), in mpm_plast.cuh

@@ -177,25 +177,32 @@ __device__ __forceinline__ float det3(const float* m) {
 }
 
 // mat3x3Inverse (matrixOps.wgsl:8-27): adjugate * (1/det); identity if det == 0.
+// The cofactors are formed in pairs (FFMA2/FMUL2); cofactors 0 and 2 equal
+// the determinant's k0 and k2 (the same products), so det3's value is
+// reproduced from them.
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ void inv3(const float* m, float* o) {
-    float det = det3(m);
+    const float2 a01 = ff2(make_float2(m[4], m[2]), make_float2(m[8], m[7]),
+                           neg2(fm2(make_float2(m[5], m[1]), make_float2(m[7], m[8]))));
+    const float2 a23 = ff2(make_float2(m[1], m[5]), make_float2(m[5], m[6]),
+                           neg2(fm2(make_float2(m[2], m[3]), make_float2(m[4], m[8]))));
+    const float k1 = ff(m[1], m[8], -fm(m[7], m[2]));
+    const float det = ff(m[6], a23.x, ff(-m[3], k1, fm(m[0], a01.x)));
     if (det == 0.0f) {
         o[0] = 1.f; o[1] = 0.f; o[2] = 0.f; o[3] = 0.f; o[4] = 1.f; o[5] = 0.f; o[6] = 0.f; o[7] = 0.f; o[8] = 1.f;
         return;
     }
-    float a0 = ff(m[4], m[8], -fm(m[5], m[7]));
-    float a1 = ff(m[2], m[7], -fm(m[1], m[8]));
-    float a2 = ff(m[1], m[5], -fm(m[2], m[4]));
-    float a3 = ff(m[5], m[6], -fm(m[3], m[8]));
-    float a4 = ff(m[0], m[8], -fm(m[2], m[6]));
-    float a5 = ff(m[2], m[3], -fm(m[0], m[5]));
-    float a6 = ff(m[3], m[7], -fm(m[4], m[6]));
-    float a7 = ff(m[1], m[6], -fm(m[0], m[7]));
-    float a8 = ff(m[0], m[4], -fm(m[1], m[3]));
-    float s = __frcp_rn(det);   // RN(1/det), the IEEE quotient 1/det
-    o[0] = fm(a0, s); o[1] = fm(a1, s); o[2] = fm(a2, s);
-    o[3] = fm(a3, s); o[4] = fm(a4, s); o[5] = fm(a5, s);
-    o[6] = fm(a6, s); o[7] = fm(a7, s); o[8] = fm(a8, s);
+    const float2 a45 = ff2(make_float2(m[0], m[2]), make_float2(m[8], m[3]),
+                           neg2(fm2(make_float2(m[2], m[0]), make_float2(m[6], m[5]))));
+    const float2 a67 = ff2(make_float2(m[3], m[1]), make_float2(m[7], m[6]),
+                           neg2(fm2(make_float2(m[4], m[0]), make_float2(m[6], m[7]))));
+    const float a8 = ff(m[0], m[4], -fm(m[1], m[3]));
+    const float s = __frcp_rn(det);   // RN(1/det), the IEEE quotient 1/det
+    const float2 s2 = dup2(s);
+    const float2 o01 = fm2(a01, s2), o23 = fm2(a23, s2), o45 = fm2(a45, s2), o67 = fm2(a67, s2);
+    o[0] = o01.x; o[1] = o01.y; o[2] = o23.x; o[3] = o23.y;
+    o[4] = o45.x; o[5] = o45.y; o[6] = o67.x; o[7] = o67.y;
+    o[8] = fm(a8, s);
 }
 
 __device__ __forceinline__ void tr3(const float* m, float* o) {
@@ -204,13 +211,18 @@ __device__ __forceinline__ void tr3(const float* m, float* o) {
     for (int i = 0; i < 9; i++) o[i] = t[i];
 }
 
+// A * B, column-major: column c, row r = A[6+r] B[3c+2] + (A[3+r] B[3c+1] + A[r] B[3c])
+// with rows 0 and 1 of each column in paired form
 __device__ __forceinline__ void mul3(const float* A, const float* B, float* o) {
     float t[9];
+    const float2 A01 = make_float2(A[0], A[1]), A34 = make_float2(A[3], A[4]), A67 = make_float2(A[6], A[7]);
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-            t[c * 3 + r] = ff(A[6 + r], B[c * 3 + 2], ff(A[3 + r], B[c * 3 + 1], fm(A[r], B[c * 3 + 0])));
+    for (int c = 0; c < 3; c++) {
+        const float2 t01 = ff2(A67, dup2(B[c * 3 + 2]), ff2(A34, dup2(B[c * 3 + 1]), fm2(A01, dup2(B[c * 3 + 0]))));
+        t[c * 3 + 0] = t01.x;
+        t[c * 3 + 1] = t01.y;
+        t[c * 3 + 2] = ff(A[8], B[c * 3 + 2], ff(A[5], B[c * 3 + 1], fm(A[2], B[c * 3 + 0])));
+    }
 #pragma unroll
     for (int i = 0; i < 9; i++) o[i] = t[i];
 }
@@ -232,10 +244,16 @@ __device__ __forceinline__ void polar3(const float* F, float* R) {
     for (int it = 0; it < 4; it++) {
         float iv[9];
         inv3(g, iv);
-        // transpose(iv)[c*3+r] = iv[r*3+c]
-        float t[9] = {iv[0], iv[3], iv[6], iv[1], iv[4], iv[7], iv[2], iv[5], iv[8]};
+        // g <- 0.5 (g + transpose(iv)), transpose(iv)[c*3+r] = iv[r*3+c], in pairs
+        const float t[9] = {iv[0], iv[3], iv[6], iv[1], iv[4], iv[7], iv[2], iv[5], iv[8]};
+        const float2 h = dup2(0.5f);
 #pragma unroll
-        for (int i = 0; i < 9; i++) g[i] = fm(0.5f, fa(g[i], t[i]));
+        for (int i = 0; i < 8; i += 2) {
+            const float2 v = fm2(h, fa2(make_float2(g[i], g[i + 1]), make_float2(t[i], t[i + 1])));
+            g[i] = v.x;
+            g[i + 1] = v.y;
+        }
+        g[8] = fm(0.5f, fa(g[8], t[8]));
     }
 #pragma unroll
     for (int i = 0; i < 9; i++) R[i] = g[i];
