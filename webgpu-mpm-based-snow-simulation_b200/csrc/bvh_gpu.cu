@@ -263,6 +263,32 @@ __global__ void k_reorder_indices(const uint32_t* __restrict__ idx, const uint32
     out[i] = idx[(size_t)order[i / 3u] * 3u + i % 3u];
 }
 
+// Bounds of each collider triangle in leaf order, from the collider buffer
+// (indices, then vertices at word num_indices + 3 v); a triangle whose index
+// points past the buffer gets infinite bounds (never skipped).
+__global__ void k_tri_boxes(const uint32_t* __restrict__ col, uint32_t words, uint32_t num_indices,
+                            float4* __restrict__ boxes) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_indices / 3u) return;
+    const float inf = __int_as_float(0x7f800000);
+    float lo[3] = {inf, inf, inf}, hi[3] = {-inf, -inf, -inf};
+    bool ok = true;
+    for (int j = 0; j < 3; j++) {
+        const size_t base = (size_t)num_indices + (size_t)col[t * 3u + j] * 3u;
+        if (base + 2u >= words) { ok = false; break; }
+        for (int k = 0; k < 3; k++) {
+            float x = __uint_as_float(col[base + k]);
+            lo[k] = fminf(lo[k], x);
+            hi[k] = fmaxf(hi[k], x);
+        }
+    }
+    if (!ok) {
+        for (int k = 0; k < 3; k++) { lo[k] = -inf; hi[k] = inf; }
+    }
+    boxes[2 * t] = make_float4(lo[0], lo[1], lo[2], 0.f);
+    boxes[2 * t + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+}
+
 uint32_t plan_nodes(uint32_t start, uint32_t count, uint32_t depth, std::vector<NodePlan>& out,
                     std::vector<uint32_t>& depth_of) {
     uint32_t id = (uint32_t)out.size();
@@ -377,6 +403,14 @@ int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t 
     *cuda_err = e;
     if (e != cudaSuccess) return MPM_ERR_CUDA;
     return herr ? MPM_ERR_ARG : MPM_OK;
+}
+
+cudaError_t triangle_boxes(const uint32_t* col_data, uint32_t words, uint32_t num_indices, float4* boxes,
+                           cudaStream_t s) {
+    const uint32_t nt = num_indices / 3u;
+    if (nt == 0) return cudaSuccess;
+    bvhg::k_tri_boxes<<<(nt + 255) / 256, 256, 0, s>>>(col_data, words, num_indices, boxes);
+    return cudaGetLastError();
 }
 
 cudaError_t reorder_indices(const uint32_t* idx, const uint32_t* order, uint32_t nt, uint32_t* out, cudaStream_t s) {

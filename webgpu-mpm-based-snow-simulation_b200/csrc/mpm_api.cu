@@ -47,6 +47,7 @@ uint32_t bvh_node_count(uint32_t nt);
 int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t n_indices, void* nodes_dev,
                      uint32_t* order_dev, cudaStream_t s, cudaError_t* cuda_err);
 cudaError_t reorder_indices(const uint32_t* idx, const uint32_t* order, uint32_t nt, uint32_t* out, cudaStream_t s);
+cudaError_t triangle_boxes(const uint32_t* col_data, uint32_t words, uint32_t num_indices, float4* boxes, cudaStream_t s);
 int mc_run(const uint32_t* density, const uint32_t* dres, const uint32_t* mres, const float* gmin, const float* gmax,
            float scale, float* out, uint32_t max_vertices, uint32_t* vertices_total, int n_sms, cudaStream_t s,
            cudaError_t* err);
@@ -71,6 +72,7 @@ struct SceneHost {
     bool have_uniforms = false;
     uint32_t* col_data = nullptr;
     uint32_t* bvh = nullptr;
+    float4* tbox = nullptr;   // per-triangle bounds (collide's early skip)
 };
 
 struct MpmMlp {
@@ -234,6 +236,7 @@ static void build_scene_dev(SceneHost& s) {
     const MpmParams& e = s.params;
     const uint32_t* col = d.col_data;
     const uint32_t* bvh = d.bvh;
+    const float4* tbox = d.tbox;
     uint32_t col_words = d.col_words, n_nodes = d.n_nodes, p_first = d.p_first, p_count = d.p_count;
     uint32_t c_nidx_override = d.c_nidx;
     std::memset(&d, 0, sizeof(d));
@@ -291,6 +294,13 @@ static void build_scene_dev(SceneHost& s) {
     d.bvh = bvh;
     d.col_words = col_words;
     d.n_nodes = n_nodes;
+    d.tbox = tbox;
+    bool ident = true;
+    for (int i = 0; i < 16; i++) {
+        float id = (i % 5 == 0) ? 1.0f : 0.0f;
+        ident = ident && d.xf[i] == id && d.xfi[i] == id;
+    }
+    d.cull = (tbox && ident) ? 1u : 0u;
     // Reciprocals RN(1/d) of the substep-constant divisors: one IEEE single
     // division each on the host, the value the oracle forms the same way.
     auto recip = [](float v) {
@@ -352,6 +362,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     for (auto& s : h->scenes) {
         if (s.col_data) cudaFree(s.col_data);
         if (s.bvh) cudaFree(s.bvh);
+        if (s.tbox) cudaFree(s.tbox);
     }
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -597,8 +608,15 @@ extern "C" int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* da
         CK(h, cudaMalloc(&s.bvh, (size_t)n_nodes * MPM_BVH_NODE_BYTES));
         CK(h, cudaMemcpy(s.bvh, nodes, (size_t)n_nodes * MPM_BVH_NODE_BYTES, cudaMemcpyHostToDevice));
     }
+    if (s.tbox) { cudaFree(s.tbox); s.tbox = nullptr; }
+    if (num_indices >= 3 && words) {
+        CK(h, cudaMalloc(&s.tbox, (size_t)(num_indices / 3) * 32));
+        CK(h, triangle_boxes(s.col_data, (uint32_t)words, num_indices, s.tbox, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
     s.dev.col_data = s.col_data;
     s.dev.bvh = s.bvh;
+    s.dev.tbox = s.tbox;
     s.dev.col_words = (uint32_t)words;
     s.dev.n_nodes = n_nodes;
     s.dev.c_nidx = num_indices;  // GpuMpmPipelineManager.ts:80 writes colliderNumIndices
@@ -631,12 +649,18 @@ extern "C" int mpm_set_collider_mesh_device(MpmHandle* h, uint32_t scene, const 
     if (r == MPM_OK && ce == cudaSuccess && n_vertices)
         ce = cudaMemcpyAsync(s.col_data + n_indices, vertices_dev, (size_t)n_vertices * 12, cudaMemcpyDeviceToDevice,
                              h->stream);
+    if (s.tbox) { cudaFree(s.tbox); s.tbox = nullptr; }
+    if (r == MPM_OK && ce == cudaSuccess && nt) {
+        ce = cudaMalloc(&s.tbox, (size_t)nt * 32);
+        if (ce == cudaSuccess) ce = triangle_boxes(s.col_data, (uint32_t)words, n_indices, s.tbox, h->stream);
+    }
     if (r == MPM_OK && ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
     if (order) cudaFree(order);
     if (r == MPM_ERR_ARG) return fail(h, MPM_ERR_ARG, "mesh index >= n_vertices (%u)", n_vertices);
     if (r != MPM_OK || ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "device BVH build: %s", cudaGetErrorString(ce));
     s.dev.col_data = s.col_data;
     s.dev.bvh = s.bvh;
+    s.dev.tbox = s.tbox;
     s.dev.col_words = (uint32_t)words;
     s.dev.n_nodes = n_nodes;
     s.dev.c_nidx = n_indices;

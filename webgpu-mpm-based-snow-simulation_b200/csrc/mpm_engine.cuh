@@ -80,6 +80,12 @@ struct SceneDev {
     uint32_t col_words, n_nodes;
     const uint32_t* col_data;
     const uint32_t* bvh;
+    // per-triangle bounds in leaf order (lo, hi as float4 pairs) and whether
+    // the collider transform is the identity: triangles whose bounds are
+    // farther from the particle than the collider threshold and clear of
+    // its path are skipped (collide)
+    const float4* tbox;
+    uint32_t cull, cull_pad;
     // reciprocals RN(1/d) of the substep-constant divisors, rounded once on
     // the host: x / d evaluates as x * RN(1/d)
     float rdt, rcd[3], rscale, rfdiv;

@@ -359,6 +359,20 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
 #pragma unroll
     for (int k = 0; k < 3; k++) { pminl[k] = fminf(curl[k], prevl[k]); pmaxl[k] = fmaxf(curl[k], prevl[k]); }
 
+    // Early skip (identity transform only): a triangle whose bounds are
+    // farther than the threshold (plus a rounding allowance) from the
+    // particle and do not meet its path can neither bring the closest
+    // distance under the threshold nor be hit by the path, so it cannot
+    // change the outcome; the other triangles run in the same order.
+    const float slack = fa(1e-4f, fm(1e-5f, fmaxf(fmaxf(fabsf(cur[0]), fabsf(cur[1])), fabsf(cur[2]))));
+    const float reach = fa(S.cthr, slack);
+    const float reach2 = fm(reach, reach);
+    float seg_lo[3], seg_hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        seg_lo[k] = fs(fminf(cur[k], prev[k]), slack);
+        seg_hi[k] = fa(fmaxf(cur[k], prev[k]), slack);
+    }
     uint32_t stack[32];
     uint32_t sp = 0;
     stack[sp++] = 0u;
@@ -380,6 +394,19 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
             for (uint32_t i = start; i < end; i++) {
                 uint32_t tb = i * 3u;
                 if (tb + 2u >= S.col_words) break;
+                if (S.cull) {
+                    const float4 blo = __ldg(S.tbox + 2 * i), bhi = __ldg(S.tbox + 2 * i + 1);
+                    const float lo3[3] = {blo.x, blo.y, blo.z}, hi3[3] = {bhi.x, bhi.y, bhi.z};
+                    float dl = 0.f;
+                    bool apart = false;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        float gap = fmaxf(0.f, fmaxf(fs(lo3[k], cur[k]), fs(cur[k], hi3[k])));
+                        dl = fa(dl, fm(gap, gap));
+                        apart = apart || seg_hi[k] < lo3[k] || seg_lo[k] > hi3[k];
+                    }
+                    if (dl > reach2 && (!do_ccd || apart)) continue;
+                }
                 float v0l[3], v1l[3], v2l[3], v0[3], v1[3], v2[3];
                 col_vertex(S, __ldg(&S.col_data[tb]), v0l);
                 col_vertex(S, __ldg(&S.col_data[tb + 1]), v1l);
