@@ -31,6 +31,8 @@ sys.path.insert(0, ROOT)
 PKG = "webgpu-mpm-based-snow-simulation_b200"
 
 METRIC = "particle-substeps/s at 4M (plain vs surrogate, agg err<=1e-3); P2G/G2P HBM GB/s"
+# learned plasticity: predicted-error threshold above which the exact map is used
+SURROGATE_UNC_THRESHOLD = 0.05
 WORKLOAD = "c2_large_pbmpm: 4,194,304-particle snow slab on 130,050-tri fBm terrain, 512^3 sparse grid, PBMPM x6, dt 5e-5"
 
 
@@ -475,7 +477,7 @@ def _timed_run(pkg, torch, spec, mode, net, tile_edge, stream, local, warmup, st
     # fixed tile storage: the pre-compacted snow spreads while it relaxes
     buf, pipe = _pipeline(pkg, spec, tile_edge, stream, local, max_tiles=6 * 4732)
     ctl = pkg.learned.PlasticityController(buf)
-    ctl.set_mode(mode, net, unc_threshold=0.05, det_threshold=1e-3, audit_fraction=0.01)
+    ctl.set_mode(mode, net, unc_threshold=SURROGATE_UNC_THRESHOLD, det_threshold=1e-3, audit_fraction=0.01)
     method = pkg.GpuSimulationMethodType.Pbmpm
     for _ in range(warmup):
         pipe.step(method, 1)

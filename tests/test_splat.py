@@ -66,3 +66,24 @@ def test_splats_edges_and_outside(gpu, oracle_mod, kind):
     want = oracle_mod.splat(kind, p, [0, 0, 0], [1, 1, 1], res, scale)
     assert np.array_equal(out.view(np.uint32), want)
     buf.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["mass", "density"])
+def test_splats_coarse_grid_aggregated(gpu, oracle_mod, kind):
+    # fewer cells than particles: the warp-aggregated form of the adds
+    p = _records(gpu, n=5000, seed=4, lo=0.1, hi=0.9)
+    spec = gpu.scenes.parity_scene(kind="explicit")
+    buf = gpu.GpuMpmBufferManager(n_particles=p.shape[0])
+    buf.write_particles(p)
+    pipe = gpu.GpuMpmPipelineManager(mpm_manager=buf, uniforms_manager=spec.uniforms)
+    res = (6, 5, 7)
+    if kind == "mass":
+        spec.uniforms.write_grid_resolution(res)
+        pipe.push_uniforms()
+    out = (buf.calculate_grid_mass(res) if kind == "mass" else buf.calculate_density(res)).cpu().numpy()
+    scale = float(np.frombuffer(spec.uniforms.bytes()[4:8], "<f4")[0])
+    want = oracle_mod.splat(kind, p, [0, 0, 0], [1, 1, 1], res, scale)
+    assert want.sum() > 0
+    assert np.array_equal(out.view(np.uint32), want)
+    buf.close()
