@@ -17,6 +17,12 @@ def _meshes(pkg):
     vq = (rng.integers(-2, 3, (400, 3)).astype(np.float32) * 0.25)
     vq[rng.random(vq.shape) < 0.1] = -0.0                  # signed zeros on the bounds
     out["ties"] = (vq, rng.integers(0, 400, (3000, 3)).astype(np.uint32))
+    # degenerate triangles: repeated vertices and zero-area slivers, equal centroids
+    vd = rng.random((50, 3)).astype(np.float32)
+    fd = rng.integers(0, 50, (600, 3)).astype(np.uint32)
+    fd[::3, 1] = fd[::3, 0]
+    fd[::5] = fd[0]
+    out["degenerate"] = (vd, fd)
     for n in (1, 4, 5, 9, 17, 1000):
         out[f"soup_{n}"] = (rng.random((3 * n, 3)).astype(np.float32), np.arange(3 * n, dtype=np.uint32).reshape(n, 3))
     return out
@@ -31,8 +37,8 @@ def test_node_count_matches_host_build(pkg):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["icosphere", "terrain_256", "ties", "soup_1", "soup_4", "soup_5", "soup_9",
-                                  "soup_17", "soup_1000"])
+@pytest.mark.parametrize("name", ["icosphere", "terrain_256", "ties", "degenerate", "soup_1", "soup_4", "soup_5",
+                                  "soup_9", "soup_17", "soup_1000"])
 def test_device_build_equals_host_build(gpu, name):
     import torch
 

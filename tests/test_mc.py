@@ -111,3 +111,22 @@ def test_mc_chain_after_simulation(gpu, oracle_mod):
     assert n == n_want and n > 30
     assert np.array_equal(mc.vertices[:n].cpu().numpy().view(np.uint32), want.view(np.uint32))
     g.close()
+
+
+@pytest.mark.gpu
+def test_mc_empty_density_gives_no_vertices(gpu):
+    import ctypes as C
+
+    import torch
+
+    spec = gpu.scenes.parity_scene(kind="explicit")
+    g = GpuScene(gpu, spec)
+    d_dev = torch.zeros((9, 10, 11), dtype=torch.int32, device="cuda")
+    out = torch.zeros((16, 6), dtype=torch.float32, device="cuda")
+    cnt, gen = C.c_uint32(7), C.c_uint32(7)
+    gpu._lib.check(gpu.load().mpm_marching_cubes(g.buf.handle, 0, C.c_void_p(d_dev.data_ptr()),
+                                                 (C.c_uint32 * 3)(11, 10, 9), (C.c_uint32 * 3)(20, 17, 13),
+                                                 C.c_void_p(out.data_ptr()), 16, C.byref(cnt), C.byref(gen)),
+                   g.buf.handle)
+    assert cnt.value == 0 and gen.value == 0
+    g.close()

@@ -109,3 +109,31 @@ def test_raymarch_chain_after_simulation(gpu, oracle_mod):
     assert np.array_equal(vol.output.cpu().numpy(), want_rgba)
     assert np.array_equal(vol.depth.cpu().numpy().view(np.uint32), want_depth.view(np.uint32))
     g.close()
+
+
+@pytest.mark.gpu
+def test_raymarch_camera_inside_grid(gpu, oracle_mod):
+    import torch
+
+    spec = gpu.scenes.parity_scene(kind="pbmpm")
+    res = (20, 20, 20)
+    spec.uniforms.write_grid_resolution(res)
+    w, h = 32, 24
+    M = inv_view_proj((0.5, 0.1, 0.45), (0.5, 0.9, 0.4), w, h)    # eye inside the unit box
+    spec.uniforms.write_view_proj_inv_mat(M.reshape(4, 4))
+    spec.uniforms.write_time(77)
+    g = GpuScene(gpu, spec)
+    vol = gpu.GpuVolumetricBufferManager(grid_resolution=res, screen_dims=(w, h))
+    grid = _blob_grid(res, seed=5)
+    vol.mass_grid.copy_(torch.from_numpy(grid.view(np.int32)))
+    vol.depth.fill_(-1.0)
+    torch.cuda.synchronize()
+    gpu.GpuVolumetricRenderPipelineManager(mpm_manager=g.buf, volumetric_manager=vol).add_raymarch_dispatch()
+    g.buf.sync()
+    scale = float(np.frombuffer(spec.uniforms.bytes()[4:8], "<f4")[0])
+    want_rgba, want_depth, want_color = oracle_mod.raymarch(grid, [0, 0, 0], [1, 1, 1], scale, M, 77, w, h)
+    assert (want_color[..., 3] > 0.05).sum() > 50
+    assert np.array_equal(vol.color.cpu().numpy().view(np.uint32), want_color.view(np.uint32))
+    assert np.array_equal(vol.output.cpu().numpy(), want_rgba)
+    assert np.array_equal(vol.depth.cpu().numpy().view(np.uint32), want_depth.view(np.uint32))
+    g.close()
