@@ -919,25 +919,15 @@ struct HaloCopy {
     uint32_t parity;
 };
 
-// Sum this tile's halo region into `cell`: the tile's own (E+2)^3 sums (one
-// TMA bulk copy) plus the overlapping parts of the neighbour halos (entries
-// of the compile-time halo table, loaded into registers in batches of U per
-// thread and added with shared i32 atomics).  The first batch of neighbour
-// loads is issued before the wait for the bulk copy, so both latencies
-// overlap.  rm_src / rm_dst (optional): the tile's stored reciprocal masses,
-// brought in by the same bulk copy.  MASS = false adds only the momentum
-// components (the mass field of the result is then undefined).  Returns false
-// (on every thread) when the copy wait ran out; the caller then stops.
-template <int E, int BS, bool MASS = true>
-__device__ __forceinline__ bool assemble_sums(const int4* tiles, const int* nbr, int4* cell, HaloCopy& hc,
-                                              const float* rm_src = nullptr, float* rm_dst = nullptr) {
+// Thread 0 issues the bulk copies of tile st's own (E+2)^3 sums (and of its
+// stored reciprocal masses when rm_dst is given) into shared memory; they
+// complete on hc's mbarrier.
+template <int E>
+__device__ __forceinline__ void halo_issue(const int4* tiles, uint32_t st, int4* cell, HaloCopy& hc,
+                                           const float* rm_src, float* rm_dst) {
     constexpr int H = E + 2, NC = H * H * H;
-    constexpr int NE = HaloEntries<E>::N;
-    constexpr int PER = (NE + BS - 1) / BS;      // entries per thread
-    constexpr int U = PER <= 10 ? PER : 8;       // entries per register batch
-    const int4* own = tiles + (size_t)nbr[13] * NC;
-    const uint32_t* tab = halo_table<E>();
     if (threadIdx.x == 0) {
+        const int4* own = tiles + (size_t)st * NC;
         // the previous tile's shared-memory reads (generic proxy) come before these writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(hc.mbar, (uint32_t)(NC * 16 + (rm_dst ? NC * 4 : 0)));
@@ -949,6 +939,27 @@ __device__ __forceinline__ bool assemble_sums(const int4* tiles, const int* nbr,
                  (uint32_t)(NC * 16) - 3 * CH, hc.mbar);
         if (rm_dst) bulk_g2s(rm_dst, rm_src, (uint32_t)(NC * 4), hc.mbar);
     }
+}
+
+// Sum this tile's halo region into `cell`: the tile's own (E+2)^3 sums (one
+// TMA bulk copy) plus the overlapping parts of the neighbour halos (entries
+// of the compile-time halo table, loaded into registers in batches of U per
+// thread and added with shared i32 atomics).  The first batch of neighbour
+// loads is issued before the wait for the bulk copy, so both latencies
+// overlap.  rm_src / rm_dst (optional): the tile's stored reciprocal masses,
+// brought in by the same bulk copy.  MASS = false adds only the momentum
+// components (the mass field of the result is then undefined).  Returns false
+// (on every thread) when the copy wait ran out; the caller then stops.
+// PRE = true: the caller issued the own-halo copies earlier (halo_issue).
+template <int E, int BS, bool MASS = true, bool PRE = false>
+__device__ __forceinline__ bool assemble_sums(const int4* tiles, const int* nbr, int4* cell, HaloCopy& hc,
+                                              const float* rm_src = nullptr, float* rm_dst = nullptr) {
+    constexpr int H = E + 2, NC = H * H * H;
+    constexpr int NE = HaloEntries<E>::N;
+    constexpr int PER = (NE + BS - 1) / BS;      // entries per thread
+    constexpr int U = PER <= 10 ? PER : 8;       // entries per register batch
+    const uint32_t* tab = halo_table<E>();
+    if (!PRE) halo_issue<E>(tiles, (uint32_t)nbr[13], cell, hc, rm_src, rm_dst);
     int4 v[U];
     int jd[U];
     auto fetch = [&](int base) {
@@ -1016,14 +1027,14 @@ __device__ __forceinline__ float4 cell_velocity_rm(const SceneDev& S, int4 s, fl
 // carry momentum only), brought into rm_s by the halo's bulk copy when rm_s
 // is given, else loaded after the assembly into the unused mass field.
 // Returns false (on every thread) when the halo copy wait ran out.
-template <int E, int BS, bool PB, int RM = 0>
+template <int E, int BS, bool PB, int RM = 0, bool PRE = false>
 __device__ __forceinline__ bool assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
                                                        const int* nbr, int4* cell, HaloCopy& hc,
                                                        float* rm_tile = nullptr, float* rm_s = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
     const bool rm_bulk = RM == 2 && rm_s != nullptr;
-    if (!assemble_sums<E, BS, RM != 2>(tiles, nbr, cell, hc, rm_bulk ? rm_tile : nullptr,
-                                       rm_bulk ? rm_s : nullptr))
+    if (!assemble_sums<E, BS, RM != 2, PRE>(tiles, nbr, cell, hc, rm_bulk ? rm_tile : nullptr,
+                                            rm_bulk ? rm_s : nullptr))
         return false;
     if (RM == 2 && !rm_bulk) {
 #pragma unroll 8
@@ -1602,14 +1613,20 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     HaloCopy hc{&mbar, 0u};
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
+    // a tile's own-halo copies are issued as soon as the previous tile's
+    // particles are done, so they overlap that tile's flush
+    if (blockIdx.x < n_st)
+        halo_issue<E>(c.tiles_b, blockIdx.x, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)blockIdx.x * NC,
+                      FIRST ? nullptr : rm_s);
     for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
         zero_mom<E>(acc);
         __syncthreads();
-        if (!assemble_velocity_tile<E, BS, true, FIRST ? 1 : 2>(c.tiles_b, S, T, nbr, cell, hc,
-                                                               c.tile_rm + (size_t)st * NC, FIRST ? nullptr : rm_s)) {
+        if (!assemble_velocity_tile<E, BS, true, FIRST ? 1 : 2, true>(c.tiles_b, S, T, nbr, cell, hc,
+                                                                     c.tile_rm + (size_t)st * NC,
+                                                                     FIRST ? nullptr : rm_s)) {
             copy_wait_failed(c, hc);
             return;
         }
@@ -1627,6 +1644,11 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
             p2g_pbmpm<E, false>(S, T, sc, mass, dxp, D, acc);
         }
         __syncthreads();
+        if (st + gridDim.x < n_st) {
+            const uint32_t nx = st + gridDim.x;
+            halo_issue<E>(c.tiles_b, nx, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)nx * NC,
+                          FIRST ? nullptr : rm_s);
+        }
         flush_mom<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
