@@ -24,7 +24,9 @@
  *   momentum / cell mass = momentum * RN(1/mass)
  *   every other division, and sqrt, are IEEE; length(v) = sqrt(dot(v,v))
  *   i32(f) = truncation toward zero, saturating, NaN -> 0
- *   exp/pow evaluated in f64 by or_exp64/or_log64 below, rounded once to f32
+ *   exp evaluated in f64 by or_exp64 below, rounded once to f32
+ *   pow evaluated in f64 by the table-driven or_log_t64/or_exp_t64 below,
+ *                  rounded once to f32
  * Every other expression follows the WGSL source's own left-to-right order;
  * the f64 instantiation uses the same formulas with IEEE f64 division.
  */
@@ -55,7 +57,6 @@ typedef OrParticle PART;
 /* ------------------------------------------------------------------ */
 uint32_t or_hash3(uint32_t x, uint32_t y, uint32_t z);
 double or_exp64(double x);
-double or_log64(double x);
 
 #if !OR_FP64
 /* xxHash32-style 3-word mix (randomNumberGenerators.wgsl:24-38). */
@@ -107,47 +108,77 @@ double or_exp64(double x) {
     return (p * pow2i(k1)) * pow2i(k2);
 }
 
-/* log(x) in f64: x = m * 2^e with m in [sqrt(1/2), sqrt(2)), then
- * log(m) = 2*atanh(s), s = (m-1)/(m+1), by its odd power series to s^23
- * (Horner in s^2 with fused multiply-adds). */
-double or_log64(double x) {
-    if (x != x || x < 0.0) return NAN;
-    if (x == 0.0) return -INFINITY;
-    if (x == INFINITY) return INFINITY;
-    int e = 0;
-    uint64_t u = d2u(x);
-    if ((u >> 52) == 0) {               /* subnormal: scale up by 2^54 */
-        x = x * 18014398509481984.0;
-        u = d2u(x);
-        e = -54;
-    }
-    e += (int)((u >> 52) & 0x7ff) - 1023;
-    double m = u2d((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull); /* [1,2) */
-    if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
-    double s = (m - 1.0) / (m + 1.0);
-    double s2 = s * s;
-    double q = 1.0 / 23.0;
-    q = fma(q, s2, 1.0 / 21.0);
-    q = fma(q, s2, 1.0 / 19.0);
-    q = fma(q, s2, 1.0 / 17.0);
-    q = fma(q, s2, 1.0 / 15.0);
-    q = fma(q, s2, 1.0 / 13.0);
-    q = fma(q, s2, 1.0 / 11.0);
-    q = fma(q, s2, 1.0 / 9.0);
-    q = fma(q, s2, 1.0 / 7.0);
-    q = fma(q, s2, 1.0 / 5.0);
-    q = fma(q, s2, 1.0 / 3.0);
-    q = fma(q, s2, 1.0);
-    const double LN2 = 6.93147180559945309417e-01;
-    return (double)e * LN2 + 2.0 * s * q;
-}
-
 float or_expf(float x) { return (float)or_exp64((double)x); }
 
-/* pow(x, y) for the one use in the step (x >= 0, y < 0): exp(y*log(x)). */
+/* The pow tables: the CUDA path reads the same generated file
+ * (webgpu-mpm-based-snow-simulation_b200/csrc/gen_pow_tables.py), so both
+ * sides hold identical constants: POW_INVC[j] = RN(1/c_j) for the slice
+ * centres c_j = 1 + (j + 1/2)/128 of [1, 2), POW_NLOGC[j] = RN(-log
+ * POW_INVC[j]), POW_EXP2[i] = RN(2^(i/64)). */
+#define MPM_POW_TABLE static const
+#include "../webgpu-mpm-based-snow-simulation_b200/csrc/mpm_pow_tables.h"
+#undef MPM_POW_TABLE
+
+static inline uint32_t f2u(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
+static inline float u2f(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
+
+/* log(x) in f64 for an f32 x > 0 (NaN for x < 0 or NaN, +inf for +inf):
+ * x = m * 2^e from the f32 fields (subnormals scaled by 2^24 first), j = the
+ * top 7 mantissa bits, r = m * POW_INVC[j] - 1 by one fma (|r| < 2^-7.9),
+ * log x = e*ln2 + POW_NLOGC[j] + log1p(r), log1p by its Taylor series to r^7
+ * (truncation < 2^-66). */
+static double or_log_t64(float x) {
+    if (!(x > 0.0f)) return NAN;
+    uint32_t u = f2u(x);
+    if (u == 0x7f800000u) return (double)x;
+    int e = -127;
+    if ((u >> 23) == 0) {
+        u = f2u(x * 0x1p24f);
+        e -= 24;
+    }
+    e += (int)(u >> 23);
+    const int j = (int)((u >> 16) & 127u);
+    const double m = (double)u2f((u & 0x7fffffu) | 0x3f800000u);
+    const double r = fma(m, POW_INVC[j], -1.0);
+    double q = fma(1.0 / 7.0, r, -1.0 / 6.0);
+    q = fma(q, r, 1.0 / 5.0);
+    q = fma(q, r, -0.25);
+    q = fma(q, r, 1.0 / 3.0);
+    q = fma(q, r, -0.5);
+    const double l1 = fma(q, r * r, r);
+    const double LN2 = 6.93147180559945309417e-01;
+    return fma((double)e, LN2, POW_NLOGC[j] + l1);
+}
+
+/* exp(z) in f64 where only its f32 rounding is used: +inf above 89 and 0
+ * below -104 (both round to the same f32 as the exact value); otherwise
+ * z = k*ln2/64 + r (Cody-Waite, k = RN(64 z / ln2), |r| <= ln2/128), e^r by
+ * its Taylor series to r^7 (truncation < 2^-73), times POW_EXP2[k mod 64]
+ * and the exact power 2^floor(k/64). */
+static double or_exp_t64(double z) {
+    if (z != z) return z;
+    if (z > 89.0) return INFINITY;
+    if (z < -104.0) return 0.0;
+    const double K = 0x1.71547652b82fep+6; /* 64 / ln2 */
+    const double L_HI = 6.93147180369123816490e-01 / 64.0, L_LO = 1.90821492927058770002e-10 / 64.0;
+    const double kf = rint(z * K);
+    const int k = (int)kf;
+    const double r = (z - kf * L_HI) - kf * L_LO;
+    double p = fma(1.0 / 5040.0, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    return (p * POW_EXP2[k & 63]) * pow2i(k >> 6);
+}
+
+/* pow(x, y) = exp(y*log(x)) in f64, rounded once to f32; pow(0, y) = +inf,
+ * 1 or 0 for y < 0, y == 0, y > 0. */
 float or_powf(float x, float y) {
     if (x == 0.0f) return y < 0.0f ? INFINITY : (y == 0.0f ? 1.0f : 0.0f);
-    return (float)or_exp64((double)y * or_log64((double)x));
+    return (float)or_exp_t64((double)y * or_log_t64(x));
 }
 
 int32_t or_f2i(float x) {

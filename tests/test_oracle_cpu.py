@@ -6,12 +6,15 @@ Python, (b) agreement of its f32 instantiation with its f64 one, (c) physical
 invariants of the transfer, and (d) the committed fixtures in tests/golden/.
 """
 import math
+import os
 import struct
 
 import numpy as np
 import pytest
 
 from helpers import compare_states, run_oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def hash3_py(x, y, z):
@@ -62,6 +65,39 @@ def test_exp_pow_error_bound(oracle_mod):
         want = math.exp(float(ys) * math.log(float(v)))
         g = L.or_powf(float(v), float(ys))
         assert abs(g - want) <= 0.51 * np.spacing(np.float32(want))
+
+
+def test_pow_matches_exact_rounding(oracle_mod):
+    """or_powf (table-driven f64 log/exp) returns the f32 nearest the exact
+    power on a sample spanning normal and subnormal bases, and keeps the
+    special cases: NaN for a negative or NaN base, pow(+inf, y<0) = 0,
+    pow(0, y<0) = +inf, pow(0, 0) = 1."""
+    from decimal import Decimal, getcontext
+    getcontext().prec = 50
+    L = oracle_mod.lib()
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([np.exp(rng.uniform(-90.0, 88.0, 1500)), rng.uniform(0.5, 2.0, 500),
+                         [1.0, 2.0, 0.5, 1e-40, 1.4e-45, 1.1754942e-38, 3e38]]).astype(np.float32)
+    for y in (f32(-0.3333333), f32(1.5), f32(1.0 / 2.2)):
+        for x in xs:
+            x = float(x)
+            ex = (Decimal(y) * Decimal(x).ln()).exp()
+            want = float("inf") if ex > Decimal("3.4028236e38") else f32(float(ex))
+            assert L.or_powf(x, y) == want, (x, y)
+    assert math.isnan(L.or_powf(float("nan"), -0.3)) and math.isnan(L.or_powf(-1.0, 0.5))
+    assert L.or_powf(float("inf"), -0.3) == 0.0 and L.or_powf(float("inf"), 0.5) == float("inf")
+    assert L.or_powf(0.0, -1.0) == float("inf") and L.or_powf(0.0, 0.0) == 1.0 and L.or_powf(0.0, 2.0) == 0.0
+
+
+def test_pow_tables_current():
+    """The committed pow tables are what gen_pow_tables.py writes."""
+    import importlib.util
+    path = os.path.join(ROOT, "webgpu-mpm-based-snow-simulation_b200", "csrc", "gen_pow_tables.py")
+    spec = importlib.util.spec_from_file_location("gen_pow_tables", path)
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    with open(gen.OUT) as f:
+        assert f.read() == gen.render()
 
 
 def test_f2i_saturates_and_truncates(oracle_mod):

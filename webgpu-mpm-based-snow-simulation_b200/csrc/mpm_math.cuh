@@ -21,7 +21,9 @@
 //   momentum / cell mass = momentum * RN(1/mass)
 //   other divisions and sqrt are IEEE
 //   i32(f): truncation toward zero, saturating, NaN -> 0
-//   exp/pow: f64 evaluation by exp64/log64 below, rounded once to f32
+//   exp: f64 evaluation by exp64 below, rounded once to f32
+//   pow: f64 evaluation by the table-driven log_t64/exp_t64 below, rounded
+//     once to f32
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -102,45 +104,71 @@ static __device__ __forceinline__ double exp64(double x) {
     return __dmul_rn(__dmul_rn(p, pow2i(k1)), pow2i(k2));
 }
 
-// log(x) in f64: x = m 2^e, m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s),
-// s = (m-1)/(m+1), odd power series to s^23 (Horner in s^2 with fused
-// multiply-adds).
-static __device__ __forceinline__ double log64(double x) {
-    if (x != x || x < 0.0) return __longlong_as_double(0x7ff8000000000000ll);
-    if (x == 0.0) return __longlong_as_double((long long)0xfff0000000000000ull);
-    if (x == __longlong_as_double(0x7ff0000000000000ll)) return x;
-    int e = 0;
-    unsigned long long u = (unsigned long long)__double_as_longlong(x);
-    if ((u >> 52) == 0) {
-        x = __dmul_rn(x, 18014398509481984.0);
-        u = (unsigned long long)__double_as_longlong(x);
-        e = -54;
+__device__ __forceinline__ float expf_m(float x) { return __double2float_rn(exp64((double)x)); }
+// Tables of log_t64 / exp_t64 (written by gen_pow_tables.py): reciprocals
+// of the 128 slice centres of [1, 2) and minus their logs, and 2^(i/64).
+// Read through the read-only data path (lanes index them divergently).
+#define MPM_POW_TABLE static __device__ const
+#include "mpm_pow_tables.h"
+#undef MPM_POW_TABLE
+
+// log(x) in f64 for an f32 x > 0 (NaN for x < 0 or NaN, +inf for +inf):
+// x = m 2^e from the f32 fields (subnormals scaled by 2^24 first), j = the
+// top 7 mantissa bits, r = m * INVC[j] - 1 (one fused multiply-add, |r| <
+// 2^-7.9), log x = e ln2 + NLOGC[j] + log1p(r), log1p by its Taylor series
+// to r^7 (truncation < 2^-66).
+static __device__ __forceinline__ double log_t64(float x) {
+    if (!(x > 0.0f)) return __longlong_as_double(0x7ff8000000000000ll);
+    uint32_t u = __float_as_uint(x);
+    if (u == 0x7f800000u) return (double)x;
+    int e = -127;
+    if ((u >> 23) == 0) {
+        u = __float_as_uint(__fmul_rn(x, 0x1p24f));
+        e -= 24;
     }
-    e += (int)((u >> 52) & 0x7ff) - 1023;
-    double m = __longlong_as_double((long long)((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull));
-    if (m > 1.4142135623730951) { m = __dmul_rn(m, 0.5); e += 1; }
-    double s = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
-    double s2 = __dmul_rn(s, s);
-    double q = 1.0 / 23.0;
-    q = __fma_rn(q, s2, 1.0 / 21.0);
-    q = __fma_rn(q, s2, 1.0 / 19.0);
-    q = __fma_rn(q, s2, 1.0 / 17.0);
-    q = __fma_rn(q, s2, 1.0 / 15.0);
-    q = __fma_rn(q, s2, 1.0 / 13.0);
-    q = __fma_rn(q, s2, 1.0 / 11.0);
-    q = __fma_rn(q, s2, 1.0 / 9.0);
-    q = __fma_rn(q, s2, 1.0 / 7.0);
-    q = __fma_rn(q, s2, 1.0 / 5.0);
-    q = __fma_rn(q, s2, 1.0 / 3.0);
-    q = __fma_rn(q, s2, 1.0);
+    e += (int)(u >> 23);
+    const int j = (int)((u >> 16) & 127u);
+    const double m = (double)__uint_as_float((u & 0x7fffffu) | 0x3f800000u);
+    const double r = __fma_rn(m, __ldg(&POW_INVC[j]), -1.0);
+    double q = __fma_rn(1.0 / 7.0, r, -1.0 / 6.0);
+    q = __fma_rn(q, r, 1.0 / 5.0);
+    q = __fma_rn(q, r, -0.25);
+    q = __fma_rn(q, r, 1.0 / 3.0);
+    q = __fma_rn(q, r, -0.5);
+    const double l1 = __fma_rn(q, __dmul_rn(r, r), r);
     const double LN2 = 6.93147180559945309417e-01;
-    return __dadd_rn(__dmul_rn((double)e, LN2), __dmul_rn(__dmul_rn(2.0, s), q));
+    return __fma_rn((double)e, LN2, __dadd_rn(__ldg(&POW_NLOGC[j]), l1));
 }
 
-__device__ __forceinline__ float expf_m(float x) { return __double2float_rn(exp64((double)x)); }
+// exp(z) in f64 where only its f32 rounding is used: +inf above 89 and 0
+// below -104 (both round to the same f32 as the exact value); otherwise
+// z = k ln2/64 + r (Cody-Waite, k = RN(64 z / ln2), |r| <= ln2/128), e^r by
+// its Taylor series to r^7 (truncation < 2^-73), times EXP2[k mod 64] and
+// the exact power 2^floor(k/64).
+static __device__ __forceinline__ double exp_t64(double z) {
+    if (z != z) return z;
+    if (z > 89.0) return __longlong_as_double(0x7ff0000000000000ll);
+    if (z < -104.0) return 0.0;
+    const double K = 0x1.71547652b82fep+6;   // 64 / ln2
+    const double L_HI = 6.93147180369123816490e-01 / 64.0, L_LO = 1.90821492927058770002e-10 / 64.0;
+    const double kf = rint(__dmul_rn(z, K));
+    const int k = (int)kf;
+    const double r = __dsub_rn(__dsub_rn(z, __dmul_rn(kf, L_HI)), __dmul_rn(kf, L_LO));
+    double p = __fma_rn(1.0 / 5040.0, r, 1.0 / 720.0);
+    p = __fma_rn(p, r, 1.0 / 120.0);
+    p = __fma_rn(p, r, 1.0 / 24.0);
+    p = __fma_rn(p, r, 1.0 / 6.0);
+    p = __fma_rn(p, r, 0.5);
+    p = __fma_rn(p, r, 1.0);
+    p = __fma_rn(p, r, 1.0);
+    return __dmul_rn(__dmul_rn(p, __ldg(&POW_EXP2[k & 63])), pow2i(k >> 6));
+}
+
+// pow(x, y) = exp(y log x) in f64, rounded once to f32; pow(0, y) = +inf,
+// 1 or 0 for y < 0, y == 0, y > 0.
 __device__ __forceinline__ float powf_m(float x, float y) {
     if (x == 0.0f) return y < 0.0f ? __int_as_float(0x7f800000) : (y == 0.0f ? 1.0f : 0.0f);
-    return __double2float_rn(exp64(__dmul_rn((double)y, log64((double)x))));
+    return __double2float_rn(exp_t64(__dmul_rn((double)y, log_t64(x))));
 }
 
 // ---- scalar f32 ops with explicit rounding (no contraction) ----------
