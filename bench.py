@@ -554,10 +554,20 @@ def surrogate_leg(pkg, args, local, stream):
                                        warm, steps)
         r_learn, rec_l, st = _timed_run(pkg, torch, spec, L.PLASTICITY_LEARNED, net, args.tile_edge, stream, local,
                                         warm, steps)
+        # control: the plain path again from the initial state with every
+        # x position moved by one ulp; its deviation from the plain run is the
+        # scene's own sensitivity (chaos floor) after the same substeps
+        import dataclasses
+        import numpy as np
+        nudged = spec.particles.copy()
+        nudged["pos"][:, 0] = np.nextafter(nudged["pos"][:, 0], np.float32(np.inf))
+        _, rec_n, _ = _timed_run(pkg, torch, dataclasses.replace(spec, particles=nudged), L.PLASTICITY_INLINE, None,
+                                 args.tile_edge, stream, local, warm, steps)
         st = {k: (int(v) if isinstance(v, int) else float(v)) for k, v in st.items()}
         out[name] = {"substeps": warm + steps, "plain": r_plain, "learned": r_learn, "vs_plain": r_learn / r_plain,
-                     "agg_rel_err_vs_plain": _agg_rel_err(_agg(rec_l), _agg(rec_p)), "stats": st}
-        del rec_p, rec_l
+                     "agg_rel_err_vs_plain": _agg_rel_err(_agg(rec_l), _agg(rec_p)),
+                     "chaos_floor_1ulp_vs_plain": _agg_rel_err(_agg(rec_n), _agg(rec_p)), "stats": st}
+        del rec_p, rec_l, rec_n
     net.close()
     return out
 
