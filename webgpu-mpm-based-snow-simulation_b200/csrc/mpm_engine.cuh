@@ -122,7 +122,9 @@ struct Counters {
     uint32_t status;     // sticky status bits
     uint32_t n_plast;    // deferred plasticity candidates of the current substep
     uint32_t step;       // substeps run on this buffer (advanced at each substep's start)
-    uint32_t pad[3];
+    uint32_t tile_ticket;  // tile kernels: tiles claimed past each CTA's first (0 between launches)
+    uint32_t tile_done;    // tile kernels: CTAs finished; the last one resets both
+    uint32_t pad;
 };
 
 struct Ctx {

@@ -550,6 +550,8 @@ __global__ void k_clear_table(Ctx c) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.counters->n_plast = 0u;
         c.counters->step += 1u;
+        c.counters->tile_ticket = 0u;
+        c.counters->tile_done = 0u;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t s = c.st_slot[i];
@@ -1385,6 +1387,27 @@ __device__ __forceinline__ uint32_t n_tiles_now(const Ctx& c) {
     return n < c.max_tiles ? n : c.max_tiles;
 }
 
+// Tile scheduling of the persistent tile kernels: CTA b takes tile b first,
+// then claims the next unclaimed tile (gridDim.x + ticket) each time it
+// finishes one, so CTAs with light tiles take more of them and a launch ends
+// within about one tile of the average.  Each tile's results go to its own
+// slots, so which CTA runs a tile changes nothing in them.  Called by thread
+// 0; the caller broadcasts the result through shared memory.
+__device__ __forceinline__ uint32_t claim_tile(const Ctx& c) {
+    return gridDim.x + atomicAdd(&c.counters->tile_ticket, 1u);
+}
+
+// A CTA leaves a tile kernel: the last one to leave zeroes the ticket for the
+// next launch (every CTA has claimed its last ticket before it counts itself).
+__device__ __forceinline__ void tiles_done(const Ctx& c) {
+    if (threadIdx.x == 0) {
+        if (atomicAdd(&c.counters->tile_done, 1u) == gridDim.x - 1u) {
+            c.counters->tile_ticket = 0u;
+            c.counters->tile_done = 0u;
+        }
+    }
+}
+
 // Neighbour table of the compact tiles, once per substep: entry st*27 + d is
 // the compact index of the tile at offset d = 9(dz+1) + 3(dy+1) + (dx+1), or
 // -1 when that tile is unoccupied or past the tile storage.
@@ -1418,9 +1441,10 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
     extern __shared__ uint4 smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ SceneDev S;
+    __shared__ uint32_t s_next;
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
-    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         zero_acc<E>(acc);
@@ -1476,9 +1500,11 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0) s_next = claim_tile(c);
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
+    tiles_done(c);
 }
 
 // ------------------------------------------------------------------
@@ -1496,9 +1522,10 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
     if (threadIdx.x == 0) mbar_init1(&mbar);
     __syncthreads();
     HaloCopy hc{&mbar, 0u};
+    __shared__ uint32_t s_next;
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
-    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
@@ -1506,6 +1533,7 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
         constexpr int NCT = (E + 2) * (E + 2) * (E + 2);
         if (!assemble_velocity_tile<E, BS, PB, RM>(c.tiles_b, S, T, nbr, cell, hc, c.tile_rm + (size_t)st * NCT)) {
             copy_wait_failed(c, hc);
+            tiles_done(c);
             return;
         }
         __syncthreads();
@@ -1523,8 +1551,10 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
             integrate(c, S, p, pid);
             store_particle(rec, p);
         }
+        if (threadIdx.x == 0) s_next = claim_tile(c);
         __syncthreads();
     }
+    tiles_done(c);
 }
 
 // ------------------------------------------------------------------
@@ -1563,9 +1593,10 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
     extern __shared__ uint4 smem_raw[];
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ SceneDev S;
+    __shared__ uint32_t s_next;
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
-    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         zero_acc<E>(acc);
@@ -1585,9 +1616,11 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
             p2g_pbmpm<E, true>(S, T, sc, p.mass, p.dxp, p.D, acc);
         }
         __syncthreads();
+        if (threadIdx.x == 0) s_next = claim_tile(c);
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
+    tiles_done(c);
 }
 
 // PBMPM iteration i>0: G2P of iteration i-1, constraints, P2G of iteration i,
@@ -1608,6 +1641,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     __shared__ SceneDev S;
     __shared__ int nbr[27];
     __shared__ uint64_t mbar;
+    __shared__ uint32_t s_next;
     if (threadIdx.x == 0) mbar_init1(&mbar);
     __syncthreads();
     HaloCopy hc{&mbar, 0u};
@@ -1618,7 +1652,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     if (blockIdx.x < n_st)
         halo_issue<E>(c.tiles_b, blockIdx.x, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)blockIdx.x * NC,
                       FIRST ? nullptr : rm_s);
-    for (uint32_t st = blockIdx.x; st < n_st; st += gridDim.x) {
+    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
@@ -1628,6 +1662,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
                                                                      c.tile_rm + (size_t)st * NC,
                                                                      FIRST ? nullptr : rm_s)) {
             copy_wait_failed(c, hc);
+            tiles_done(c);
             return;
         }
         __syncthreads();
@@ -1644,14 +1679,17 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
             p2g_pbmpm<E, false>(S, T, sc, mass, dxp, D, acc);
         }
         __syncthreads();
-        if (st + gridDim.x < n_st) {
-            const uint32_t nx = st + gridDim.x;
-            halo_issue<E>(c.tiles_b, nx, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)nx * NC,
-                          FIRST ? nullptr : rm_s);
+        if (threadIdx.x == 0) {
+            const uint32_t nx = claim_tile(c);
+            s_next = nx;
+            if (nx < n_st)
+                halo_issue<E>(c.tiles_b, nx, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)nx * NC,
+                              FIRST ? nullptr : rm_s);
         }
         flush_mom<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
+    tiles_done(c);
 }
 
 // ------------------------------------------------------------------
