@@ -58,7 +58,7 @@ using namespace mpm;
 static const char* kKernelNames[K_COUNT] = {
     "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
     "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense",
-    "tile_nbr", "plasticity"};
+    "tile_nbr", "plasticity", "tile_order"};
 
 struct TimedLaunch {
     uint32_t kid;
@@ -127,6 +127,7 @@ struct MpmHandle {
     int4* tiles[3] = {nullptr, nullptr, nullptr};   // first transfer, then the PBMPM iterations' ping-pong
     float* tile_rm = nullptr;     // max_tiles x (E+2)^3 reciprocal cell masses
     int32_t* st_nbr = nullptr;    // max_tiles x 27 neighbour indices
+    uint32_t* tile_order = nullptr;  // max_tiles: the tile kernels' claim order
     // deferred / learned plasticity
     int plast_mode = PLAST_INLINE;
     MpmMlp* mlp = nullptr;
@@ -354,7 +355,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
                     h->tiles[0], h->tiles[1], h->tiles[2], h->tile_rm, h->d_scenes, h->d_scene_first, h->counters,
-                    h->iter_rec, h->st_nbr,
+                    h->iter_rec, h->st_nbr, h->tile_order,
                     h->plast_list, h->d_stats, h->d_pair_count};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -402,12 +403,14 @@ static int alloc_tiles(MpmHandle* h, uint32_t n) {
     for (int i = 0; i < 3; i++)
         if (h->tiles[i]) { cudaFree(h->tiles[i]); h->tiles[i] = nullptr; }
     if (h->st_nbr) { cudaFree(h->st_nbr); h->st_nbr = nullptr; }
+    if (h->tile_order) { cudaFree(h->tile_order); h->tile_order = nullptr; }
     if (h->tile_rm) { cudaFree(h->tile_rm); h->tile_rm = nullptr; }
     size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     h->max_tiles = n;
     for (int i = 0; i < 3; i++) CK(h, cudaMalloc(&h->tiles[i], (size_t)n * NC * 16));
     CK(h, cudaMalloc(&h->tile_rm, (size_t)n * NC * 4));
     CK(h, cudaMalloc(&h->st_nbr, (size_t)n * 27 * 4));
+    CK(h, cudaMalloc(&h->tile_order, (size_t)n * 4));
     destroy_graphs(h);
     return MPM_OK;
 }
@@ -729,6 +732,7 @@ static Ctx make_ctx(MpmHandle* h, int parity) {
     c.tiles_b = h->tiles[0];
     c.iter_rec = h->iter_rec;
     c.st_nbr = h->st_nbr;
+    c.tile_order = h->tile_order;
     c.tile_rm = h->tile_rm;
     c.plast_list = h->plast_list;
     c.plast_defer = h->plast_mode != PLAST_INLINE ? 1u : 0u;
@@ -818,11 +822,16 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
     L(K_COMPACT_C);
     L(K_BIN_SCATTER);
     L(K_TILE_NBR);
+    L(K_TILE_ORDER);
+    // each tile pass claims the tile order from the other end than the pass
+    // before it (which wrote the tiles it reads)
+    c.order_rev = 0u;
     if (method == MPM_METHOD_EXPLICIT) {
         c.tiles_a = h->tiles[0];
         L(K_P2G_EXPLICIT);
         if (stop_p2g) { h->last_tiles = 0; return cudaSuccess; }
         c.tiles_b = h->tiles[0];
+        c.order_rev = 1u;
         L(K_G2P_EXPLICIT);
         if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = 0;
@@ -839,11 +848,13 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
             c.tiles_b = h->tiles[cur];
             c.tiles_a = h->tiles[nxt];
             c.iter_first = it == 1 ? 1u : 0u;
+            c.order_rev = it & 1u;
             L(K_PBMPM_ITER);
             cur = nxt;
         }
         c.tiles_b = h->tiles[cur];
         c.g2p_rm = n_iter > 1 ? 1u : 0u;
+        c.order_rev = n_iter & 1u;
         L(K_G2P_PBMPM);
         if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = cur;

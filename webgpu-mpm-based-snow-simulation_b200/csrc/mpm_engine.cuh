@@ -147,6 +147,9 @@ struct Ctx {
     int4* tiles_b;            // tiles read by this pass's G2P
     float4* iter_rec;         // PBMPM iteration records, IR_PLANES x n float4, sorted order
     int32_t* st_nbr;          // per compact tile, the compact index of its 27 neighbours (-1: none)
+    uint32_t* tile_order;     // optional: the order the tile kernels claim tiles in (Morton order of
+                              // the tile coordinates, per scene); nullptr: compact index order
+    uint32_t order_rev;       // this launch claims tile_order from its end (alternates per launch)
     float* tile_rm;           // per tile (E+2)^3 reciprocal cell masses of the substep (PBMPM iterations)
     const int4* tiles_m;      // readback only: tiles holding the substep's mass sums (nullptr: tiles_b)
     uint32_t iter_first;      // this PBMPM iteration forms and stores the reciprocal masses
@@ -188,6 +191,7 @@ enum KernelId : uint32_t {
     K_GRID_DENSE,
     K_TILE_NBR,
     K_PLASTICITY,
+    K_TILE_ORDER,
     K_COUNT
 };
 

@@ -1387,14 +1387,87 @@ __device__ __forceinline__ uint32_t n_tiles_now(const Ctx& c) {
     return n < c.max_tiles ? n : c.max_tiles;
 }
 
-// Tile scheduling of the persistent tile kernels: CTA b takes tile b first,
-// then claims the next unclaimed tile (gridDim.x + ticket) each time it
-// finishes one, so CTAs with light tiles take more of them and a launch ends
-// within about one tile of the average.  Each tile's results go to its own
-// slots, so which CTA runs a tile changes nothing in them.  Called by thread
-// 0; the caller broadcasts the result through shared memory.
-__device__ __forceinline__ uint32_t claim_tile(const Ctx& c) {
-    return gridDim.x + atomicAdd(&c.counters->tile_ticket, 1u);
+// Tile scheduling of the persistent tile kernels: CTA b takes claim slot b
+// first, then the next unclaimed slot (gridDim.x + ticket) each time it
+// finishes a tile, so CTAs with light tiles take more of them and a launch
+// ends within about one tile of the average.  Slot k maps to a tile through
+// tile_order (Morton order, so the tiles in flight at one time are neighbours
+// and share their halo data in L2; read from its end on alternate launches,
+// so a launch starts on the tiles the previous one wrote last).  Each tile's
+// results go to its own slots, so which CTA runs a tile, and when, changes
+// nothing in them.  Returns n (stop) past the last slot.
+__device__ __forceinline__ uint32_t tile_at(const Ctx& c, uint32_t k, uint32_t n) {
+    if (k >= n) return n;
+    if (!c.tile_order) return k;
+    const uint32_t st = __ldg(c.tile_order + (c.order_rev ? n - 1u - k : k));
+    return st < n ? st : n;
+}
+
+// Called by thread 0; the caller broadcasts the result through shared memory.
+__device__ __forceinline__ uint32_t claim_tile(const Ctx& c, uint32_t n) {
+    return tile_at(c, gridDim.x + atomicAdd(&c.counters->tile_ticket, 1u), n);
+}
+
+// Claim order of the tiles: a bitonic sort in one CTA of the keys
+// (scene << 48 | Morton code of the biased 16-bit tile coordinates) of up to
+// TILE_ORDER_CAP tiles; more tiles keep the compact index order.  The sort
+// only swaps (key, index) pairs, so the result is always a permutation.
+constexpr uint32_t TILE_ORDER_CAP = 8192;
+constexpr size_t TILE_ORDER_SMEM = TILE_ORDER_CAP * (8 + 2);
+
+__device__ __forceinline__ uint64_t spread3_16(uint32_t v) {
+    uint64_t x = v & 0xffffu;
+    x = (x | (x << 32)) & 0x1f00000000ffffull;
+    x = (x | (x << 16)) & 0x1f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
+    extern __shared__ uint4 smem_raw[];
+    uint64_t* key = reinterpret_cast<uint64_t*>(smem_raw);
+    uint16_t* idx = reinterpret_cast<uint16_t*>(key + TILE_ORDER_CAP);
+    const uint32_t n = n_tiles_now(c);
+    if (n > TILE_ORDER_CAP) {
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) c.tile_order[i] = i;
+        return;
+    }
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
+        uint64_t k = ~0ull;
+        if (i < n) {
+            const uint64_t t = c.st_key[i];
+            const uint64_t m = spread3_16((uint32_t)(t >> 32)) | (spread3_16((uint32_t)(t >> 16)) << 1) |
+                               (spread3_16((uint32_t)t) << 2);
+            k = ((t >> 48) << 48) | m;
+            if (k == ~0ull) k -= 1;   // padding sorts last
+        }
+        key[i] = k;
+        idx[i] = (uint16_t)i;
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= n2; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
+                const uint32_t p = i ^ j;
+                if (p > i) {
+                    const bool up = (i & k) == 0;
+                    const uint64_t a = key[i], b = key[p];
+                    if ((a > b) == up) {
+                        key[i] = b;
+                        key[p] = a;
+                        const uint16_t t = idx[i];
+                        idx[i] = idx[p];
+                        idx[p] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) c.tile_order[i] = idx[i];
 }
 
 // A CTA leaves a tile kernel: the last one to leave zeroes the ticket for the
@@ -1444,7 +1517,7 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
     __shared__ uint32_t s_next;
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
-    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
+    for (uint32_t st = tile_at(c, blockIdx.x, n_st); st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         zero_acc<E>(acc);
@@ -1500,7 +1573,7 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_next = claim_tile(c);
+        if (threadIdx.x == 0) s_next = claim_tile(c, n_st);
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
@@ -1525,7 +1598,7 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
     __shared__ uint32_t s_next;
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
-    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
+    for (uint32_t st = tile_at(c, blockIdx.x, n_st); st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
@@ -1551,7 +1624,7 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
             integrate(c, S, p, pid);
             store_particle(rec, p);
         }
-        if (threadIdx.x == 0) s_next = claim_tile(c);
+        if (threadIdx.x == 0) s_next = claim_tile(c, n_st);
         __syncthreads();
     }
     tiles_done(c);
@@ -1596,7 +1669,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
     __shared__ uint32_t s_next;
     uint32_t cur_scene = INVALID;
     uint32_t n_st = n_tiles_now(c);
-    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
+    for (uint32_t st = tile_at(c, blockIdx.x, n_st); st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         zero_acc<E>(acc);
@@ -1616,7 +1689,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
             p2g_pbmpm<E, true>(S, T, sc, p.mass, p.dxp, p.D, acc);
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_next = claim_tile(c);
+        if (threadIdx.x == 0) s_next = claim_tile(c, n_st);
         flush_tile<E>(acc, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
@@ -1649,10 +1722,11 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     uint32_t n_st = n_tiles_now(c);
     // a tile's own-halo copies are issued as soon as the previous tile's
     // particles are done, so they overlap that tile's flush
-    if (blockIdx.x < n_st)
-        halo_issue<E>(c.tiles_b, blockIdx.x, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)blockIdx.x * NC,
+    const uint32_t st0 = tile_at(c, blockIdx.x, n_st);
+    if (st0 < n_st)
+        halo_issue<E>(c.tiles_b, st0, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)st0 * NC,
                       FIRST ? nullptr : rm_s);
-    for (uint32_t st = blockIdx.x; st < n_st; st = s_next) {
+    for (uint32_t st = st0; st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
@@ -1680,7 +1754,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            const uint32_t nx = claim_tile(c);
+            const uint32_t nx = claim_tile(c, n_st);
             s_next = nx;
             if (nx < n_st)
                 halo_issue<E>(c.tiles_b, nx, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)nx * NC,
@@ -1845,7 +1919,7 @@ cudaError_t configure_tile_kernels(int* blocks_per_sm) {
         }
         blocks_per_sm[kid] = nb_min > 0 ? nb_min : 1;
     }
-    return cudaSuccess;
+    return cudaFuncSetAttribute(k_tile_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_ORDER_SMEM);
 }
 
 template <int E>
@@ -1874,6 +1948,7 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
             else k_g2p_integrate<E, true, BS_DEFAULT, 0><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c);
             break;
         case K_GRID_DENSE: k_grid_dense<E><<<grid_tiles, 256, 0, s>>>(c, scene, apply, out); break;
+        case K_TILE_ORDER: if (c.tile_order) k_tile_order<<<1, 1024, TILE_ORDER_SMEM, s>>>(c); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
