@@ -1408,66 +1408,71 @@ __device__ __forceinline__ uint32_t claim_tile(const Ctx& c, uint32_t n) {
     return tile_at(c, gridDim.x + atomicAdd(&c.counters->tile_ticket, 1u), n);
 }
 
-// Claim order of the tiles: a bitonic sort in one CTA of the keys
-// (scene << 48 | Morton code of the biased 16-bit tile coordinates) of up to
-// TILE_ORDER_CAP tiles; more tiles keep the compact index order.  The sort
-// only swaps (key, index) pairs, so the result is always a permutation.
-constexpr uint32_t TILE_ORDER_CAP = 8192;
-constexpr size_t TILE_ORDER_SMEM = TILE_ORDER_CAP * (8 + 2);
+// Claim order of the tiles: a counting sort in one CTA by a 15-bit Morton
+// bucket of the tile coordinates (5 low bits per axis, offset per scene), so
+// the tiles of a 32^3-tile neighbourhood are ordered along the Morton curve
+// (tiles in one bucket keep an arbitrary order).  The scatter positions are
+// the buckets' prefix offsets, so the result is always a permutation.
+constexpr uint32_t TILE_ORDER_BUCKETS = 1u << 15;
+constexpr size_t TILE_ORDER_SMEM = TILE_ORDER_BUCKETS * 4;
 
-__device__ __forceinline__ uint64_t spread3_16(uint32_t v) {
-    uint64_t x = v & 0xffffu;
-    x = (x | (x << 32)) & 0x1f00000000ffffull;
-    x = (x | (x << 16)) & 0x1f0000ff0000ffull;
-    x = (x | (x << 8)) & 0x100f00f00f00f00full;
-    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
-    x = (x | (x << 2)) & 0x1249249249249249ull;
+__device__ __forceinline__ uint32_t spread3_5(uint32_t v) {
+    uint32_t x = v & 31u;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
     return x;
+}
+
+__device__ __forceinline__ uint32_t tile_bucket(uint64_t key) {
+    const uint32_t m = spread3_5((uint32_t)(key >> 32)) | (spread3_5((uint32_t)(key >> 16)) << 1) |
+                       (spread3_5((uint32_t)key) << 2);
+    return (m + (uint32_t)(key >> 48) * 0x9E3779B1u) & (TILE_ORDER_BUCKETS - 1u);
 }
 
 __global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
     extern __shared__ uint4 smem_raw[];
-    uint64_t* key = reinterpret_cast<uint64_t*>(smem_raw);
-    uint16_t* idx = reinterpret_cast<uint16_t*>(key + TILE_ORDER_CAP);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
+    __shared__ uint32_t warp_sum[32];
+    constexpr uint32_t PER = TILE_ORDER_BUCKETS / 1024;   // buckets per thread
     const uint32_t n = n_tiles_now(c);
-    if (n > TILE_ORDER_CAP) {
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) c.tile_order[i] = i;
-        return;
+    for (uint32_t b = threadIdx.x; b < TILE_ORDER_BUCKETS; b += 1024) hist[b] = 0u;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += 1024) atomicAdd(&hist[tile_bucket(c.st_key[i])], 1u);
+    __syncthreads();
+    // exclusive prefix sums: each thread scans its PER consecutive buckets,
+    // the thread totals are scanned across the block
+    const uint32_t b0 = threadIdx.x * PER;
+    uint32_t tot = 0;
+    for (uint32_t k = 0; k < PER; k++) tot += hist[b0 + k];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = tot;
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += v;
     }
-    uint32_t n2 = 1;
-    while (n2 < n) n2 <<= 1;
-    for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
-        uint64_t k = ~0ull;
-        if (i < n) {
-            const uint64_t t = c.st_key[i];
-            const uint64_t m = spread3_16((uint32_t)(t >> 32)) | (spread3_16((uint32_t)(t >> 16)) << 1) |
-                               (spread3_16((uint32_t)t) << 2);
-            k = ((t >> 48) << 48) | m;
-            if (k == ~0ull) k -= 1;   // padding sorts last
+    if (lane == 31u) warp_sum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_sum[lane], wi = w;
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, wi, d);
+            if (lane >= d) wi += v;
         }
-        key[i] = k;
-        idx[i] = (uint16_t)i;
+        warp_sum[lane] = wi - w;   // exclusive over warps
     }
     __syncthreads();
-    for (uint32_t k = 2; k <= n2; k <<= 1)
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
-                const uint32_t p = i ^ j;
-                if (p > i) {
-                    const bool up = (i & k) == 0;
-                    const uint64_t a = key[i], b = key[p];
-                    if ((a > b) == up) {
-                        key[i] = b;
-                        key[p] = a;
-                        const uint16_t t = idx[i];
-                        idx[i] = idx[p];
-                        idx[p] = t;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) c.tile_order[i] = idx[i];
+    uint32_t run = warp_sum[warp] + inc - tot;
+    for (uint32_t k = 0; k < PER; k++) {
+        const uint32_t h = hist[b0 + k];
+        hist[b0 + k] = run;
+        run += h;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += 1024) {
+        const uint32_t pos = atomicAdd(&hist[tile_bucket(c.st_key[i])], 1u);
+        if (pos < n) c.tile_order[pos] = i;
+    }
 }
 
 // A CTA leaves a tile kernel: the last one to leave zeroes the ticket for the
