@@ -1415,6 +1415,7 @@ __device__ __forceinline__ uint32_t claim_tile(const Ctx& c, uint32_t n) {
 // the buckets' prefix offsets, so the result is always a permutation.
 constexpr uint32_t TILE_ORDER_BUCKETS = 1u << 15;
 constexpr size_t TILE_ORDER_SMEM = TILE_ORDER_BUCKETS * 4;
+constexpr uint32_t TILE_ORDER_MIN = 1024;   // at most this many tiles keep the compact order
 
 __device__ __forceinline__ uint32_t spread3_5(uint32_t v) {
     uint32_t x = v & 31u;
@@ -1436,6 +1437,11 @@ __global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
     __shared__ uint32_t warp_sum[32];
     constexpr uint32_t PER = TILE_ORDER_BUCKETS / 1024;   // buckets per thread
     const uint32_t n = n_tiles_now(c);
+    if (n <= TILE_ORDER_MIN) {
+        // few tiles: nearly all run at once, so their order gains nothing
+        for (uint32_t i = threadIdx.x; i < n; i += 1024) c.tile_order[i] = i;
+        return;
+    }
     for (uint32_t b = threadIdx.x; b < TILE_ORDER_BUCKETS; b += 1024) hist[b] = 0u;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += 1024) atomicAdd(&hist[tile_bucket(c.st_key[i])], 1u);
