@@ -1408,14 +1408,15 @@ __device__ __forceinline__ uint32_t claim_tile(const Ctx& c, uint32_t n) {
     return tile_at(c, gridDim.x + atomicAdd(&c.counters->tile_ticket, 1u), n);
 }
 
-// Claim order of the tiles: a counting sort in one CTA by a 15-bit Morton
-// bucket of the tile coordinates (5 low bits per axis, offset per scene), so
-// the tiles of a 32^3-tile neighbourhood are ordered along the Morton curve
+// Claim order of the tiles: a counting sort in one CTA by a 12- or 15-bit
+// Morton bucket of the tile coordinates (4 or 5 low bits per axis, offset per
+// scene), so the tiles of a 16^3- or 32^3-tile neighbourhood are ordered along
+// the Morton curve
 // (tiles in one bucket keep an arbitrary order).  The scatter positions are
 // the buckets' prefix offsets, so the result is always a permutation.
 constexpr uint32_t TILE_ORDER_BUCKETS = 1u << 15;
 constexpr size_t TILE_ORDER_SMEM = TILE_ORDER_BUCKETS * 4;
-constexpr uint32_t TILE_ORDER_MIN = 1024;   // at most this many tiles keep the compact order
+constexpr uint32_t TILE_ORDER_MIN = 256;    // at most this many tiles keep the compact order
 
 __device__ __forceinline__ uint32_t spread3_5(uint32_t v) {
     uint32_t x = v & 31u;
@@ -1425,31 +1426,28 @@ __device__ __forceinline__ uint32_t spread3_5(uint32_t v) {
     return x;
 }
 
-__device__ __forceinline__ uint32_t tile_bucket(uint64_t key) {
-    const uint32_t m = spread3_5((uint32_t)(key >> 32)) | (spread3_5((uint32_t)(key >> 16)) << 1) |
-                       (spread3_5((uint32_t)key) << 2);
-    return (m + (uint32_t)(key >> 48) * 0x9E3779B1u) & (TILE_ORDER_BUCKETS - 1u);
+// bucket of a tile key: the Morton code of the low `bits` bits of each
+// coordinate (bits = 4 or 5), offset per scene, modulo nb = 2^(3 bits)
+__device__ __forceinline__ uint32_t tile_bucket(uint64_t key, uint32_t axis_mask, uint32_t nb) {
+    const uint32_t m = spread3_5((uint32_t)(key >> 32) & axis_mask) |
+                       (spread3_5((uint32_t)(key >> 16) & axis_mask) << 1) |
+                       (spread3_5((uint32_t)key & axis_mask) << 2);
+    return (m + (uint32_t)(key >> 48) * 0x9E3779B1u) & (nb - 1u);
 }
 
-__global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
-    extern __shared__ uint4 smem_raw[];
-    uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
-    __shared__ uint32_t warp_sum[32];
-    constexpr uint32_t PER = TILE_ORDER_BUCKETS / 1024;   // buckets per thread
-    const uint32_t n = n_tiles_now(c);
-    if (n <= TILE_ORDER_MIN) {
-        // few tiles: nearly all run at once, so their order gains nothing
-        for (uint32_t i = threadIdx.x; i < n; i += 1024) c.tile_order[i] = i;
-        return;
-    }
-    for (uint32_t b = threadIdx.x; b < TILE_ORDER_BUCKETS; b += 1024) hist[b] = 0u;
+template <uint32_t BITS>
+__device__ __forceinline__ void tile_order_sort(const Ctx& c, uint32_t n, uint32_t* hist, uint32_t* warp_sum) {
+    constexpr uint32_t NB = 1u << (3 * BITS), PER = NB / 1024u;   // buckets, buckets per thread
+    constexpr uint32_t AXIS = (1u << BITS) - 1u;
+    for (uint32_t b = threadIdx.x; b < NB; b += 1024) hist[b] = 0u;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += 1024) atomicAdd(&hist[tile_bucket(c.st_key[i])], 1u);
+    for (uint32_t i = threadIdx.x; i < n; i += 1024) atomicAdd(&hist[tile_bucket(c.st_key[i], AXIS, NB)], 1u);
     __syncthreads();
     // exclusive prefix sums: each thread scans its PER consecutive buckets,
     // the thread totals are scanned across the block
     const uint32_t b0 = threadIdx.x * PER;
     uint32_t tot = 0;
+#pragma unroll
     for (uint32_t k = 0; k < PER; k++) tot += hist[b0 + k];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t inc = tot;
@@ -1469,6 +1467,7 @@ __global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
     }
     __syncthreads();
     uint32_t run = warp_sum[warp] + inc - tot;
+#pragma unroll
     for (uint32_t k = 0; k < PER; k++) {
         const uint32_t h = hist[b0 + k];
         hist[b0 + k] = run;
@@ -1476,9 +1475,24 @@ __global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += 1024) {
-        const uint32_t pos = atomicAdd(&hist[tile_bucket(c.st_key[i])], 1u);
+        const uint32_t pos = atomicAdd(&hist[tile_bucket(c.st_key[i], AXIS, NB)], 1u);
         if (pos < n) c.tile_order[pos] = i;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
+    extern __shared__ uint4 smem_raw[];
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
+    __shared__ uint32_t warp_sum[32];
+    const uint32_t n = n_tiles_now(c);
+    if (n <= TILE_ORDER_MIN) {
+        // few tiles: nearly all run at once, so their order gains nothing
+        for (uint32_t i = threadIdx.x; i < n; i += 1024) c.tile_order[i] = i;
+        return;
+    }
+    // up to 4,096 tiles: 4 bits per axis (4,096 buckets), else 5 (32,768)
+    if (n <= 4096u) tile_order_sort<4>(c, n, hist, warp_sum);
+    else tile_order_sort<5>(c, n, hist, warp_sum);
 }
 
 // A CTA leaves a tile kernel: the last one to leave zeroes the ticket for the
