@@ -1411,10 +1411,10 @@ __device__ __forceinline__ uint32_t claim_tile(const Ctx& c, uint32_t n) {
 // Claim order of the tiles: a counting sort in one CTA by a 12- or 15-bit
 // Morton bucket of the tile coordinates (4 or 5 low bits per axis, offset per
 // scene), so the tiles of a 16^3- or 32^3-tile neighbourhood are ordered along
-// the Morton curve
-// (tiles in one bucket keep an arbitrary order).  The scatter positions are
-// the buckets' prefix offsets, so the result is always a permutation.
-constexpr uint32_t TILE_ORDER_BUCKETS = 1u << 15;
+// the Morton curve (tiles in one bucket keep an arbitrary order).  The scatter
+// positions are the buckets' prefix offsets, so the result is always a
+// permutation.
+constexpr uint32_t TILE_ORDER_BUCKETS = 1u << 15;   // the wider bucket count
 constexpr size_t TILE_ORDER_SMEM = TILE_ORDER_BUCKETS * 4;
 constexpr uint32_t TILE_ORDER_MIN = 256;    // at most this many tiles keep the compact order
 
