@@ -362,11 +362,16 @@ int mpm_get_plasticity_stats(MpmHandle* h, MpmPlasticityStats* out, int reset);
  * one array and clears what must start empty, so calls whose work overlaps
  * on the GPU (different streams, or other host threads, on one device) race
  * and must be serialised by the caller.  Work is enqueued on `stream`
- * (NULL: the legacy default stream).  If status_out is non-NULL the call
- * waits for the stream, stores the device status bits and returns
- * MPM_ERR_DEVICE_STATUS when any is set.  err (err_len bytes, may be NULL)
- * receives a message on failure.  The calling thread's current device is
- * restored on return. */
+ * (NULL: the legacy default stream); the scene record travels as a kernel
+ * argument, so with status_out NULL the call returns without waiting for the
+ * GPU and the device status is not reported.  If status_out is non-NULL the
+ * call waits for the stream, stores the device status bits and returns
+ * MPM_ERR_DEVICE_STATUS when any is set.  The collider query tests every
+ * triangle of a leaf it reaches: the per-triangle bounds a handle uses to
+ * skip distant triangles would need an allocation, so this path does without
+ * them (same results, slower on large meshes).  err (err_len bytes, may be
+ * NULL) receives a message on failure.  The calling thread's current device
+ * is restored on return. */
 #define MPM_NOALLOC_MAX_PARTICLES 65536u
 #define MPM_NOALLOC_MAX_TILES 512u
 #define MPM_NOALLOC_TILE_EDGE 8u

@@ -1,0 +1,191 @@
+"""The benchmark scenes in their own mode, against the oracle.
+
+The benchmark configurations run the step with constants that differ from the
+reference's: y-up gravity (0, -9.8, 0), hardening 10, a grid-side sticky
+ground layer with slip walls (boundary mode 1), collider margins scaled to the
+cell size, and fixed-point scales of 2^34 (config 0), 2^39 (config 1) and 2^45
+(config 2).  Each scene here is advanced on the GPU through the C ABI and by
+the f32 oracle from the same initial records, in that mode.
+
+Bar: the fixed-point grid and every particle field bit for bit after one
+substep, the particle fields bit for bit after 20 substeps; against the f64
+oracle, after 100 substeps of config 0, the centre of mass (relative to its
+own magnitude), the net momentum (relative to the total absolute momentum) and
+the mean J_p (relative to itself) each within 1e-3.
+"""
+import numpy as np
+import pytest
+
+from helpers import GpuScene, compare_states
+
+pytestmark = pytest.mark.gpu
+
+AGG_TOL = 1e-3
+
+
+def _oracle(oracle_mod, spec, n_steps, fp64=False, stop_after=0):
+    """Oracle context and records after n_steps substeps (capacities sized for
+    the large slab's ~3e5 reference blocks)."""
+    p = spec.particles.copy()
+    if fp64:
+        p = oracle_mod.to_fp64(p)
+    o = oracle_mod.Oracle(p.shape[0], max_blocks=600000, hash_size=2000003, fp64=fp64)
+    if spec.mesh is not None:
+        o.set_collider(*spec.mesh)
+    for _ in range(n_steps):
+        o.step(spec.uniforms.bytes(), spec.params, p, spec.method, stop_after)
+    return o, p
+
+
+def _aggregates(rec):
+    """(centre of mass, net momentum, total |momentum|, mean J_p) in f64, for
+    192-byte records or the f64 oracle's records."""
+    m = rec["mass"].astype(np.float64)
+    v = rec["vel"].astype(np.float64)
+    com = (rec["pos"].astype(np.float64) * m[:, None]).sum(0) / m.sum()
+    mom = (v * m[:, None]).sum(0)
+    abs_mom = float((np.linalg.norm(v, axis=1) * m).sum())
+    Fp = rec["Fp"]
+    Fp = Fp.reshape(-1, 3, 3) if Fp.ndim == 2 else Fp[:, :, :3]
+    jp = float(np.linalg.det(Fp.astype(np.float64)).mean())
+    return com, mom, abs_mom, jp
+
+
+def _agg_errors(got, ref64):
+    a, b = _aggregates(got), _aggregates(ref64)
+    return {"centre_of_mass": float(np.abs(a[0] - b[0]).max() / np.abs(b[0]).max()),
+            "momentum": float(np.abs(a[1] - b[1]).max() / max(b[2], 1e-30)),
+            "mean_jp": float(abs(a[3] - b[3]) / abs(b[3]))}
+
+
+def _config_mode(spec):
+    """The scene really runs in the benchmark mode (guards the fixtures)."""
+    p = spec.params
+    assert p["boundary_mode"] == 1 and p["ground_axis"] == 1
+    assert list(p["gravity"]) == [0.0, -9.8, 0.0]
+    assert p["hardening_explicit"] == 10.0 and p["hardening_pbmpm"] == 10.0
+
+
+def _c0(gpu):
+    return gpu.scenes.c0_explicit_snow()
+
+
+def _c1(gpu):
+    return gpu.scenes.c1_pbmpm_spheres()
+
+
+def _c2_block(gpu):
+    return gpu.scenes.c2_large_pbmpm(counts=(128, 32, 128))
+
+
+SCENES = {"c0": _c0, "c1": _c1, "c2_block": _c2_block}
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_config_one_substep_grid_and_particles_bit_exact(gpu, oracle_mod, name):
+    spec = SCENES[name](gpu)
+    _config_mode(spec)
+    g = GpuScene(gpu, spec)
+    assert g.step(1) == 0
+    got = g.particles()
+    o, want = _oracle(oracle_mod, spec, 1)
+    compare_states(got, want)
+    if max(spec.res) <= 128:
+        grid_gpu = g.grid(apply_update=(spec.method == 0))
+        grid_ref = o.dense_grid(spec.uniforms.bytes())
+        assert np.count_nonzero(grid_ref[..., 0]) > 1000
+        assert np.array_equal(grid_gpu, grid_ref), f"{np.count_nonzero(grid_gpu != grid_ref)} cells differ"
+    o.close()
+    g.close()
+
+
+def test_config2_block_p2g_grid_bit_exact(gpu, oracle_mod):
+    """The large slab's first transfer at its 512^3 grid and 2^45 scale: the
+    dense grid is compared over the slab's bounding box of cells."""
+    spec = _c2_block(gpu)
+    _config_mode(spec)
+    g = GpuScene(gpu, spec)
+    assert g.p2g_only() == 0
+    grid_gpu = g.grid()
+    o, _ = _oracle(oracle_mod, spec, 1, stop_after=1)
+    grid_ref = o.dense_grid(spec.uniforms.bytes())
+    occupied = np.count_nonzero(grid_ref[..., 0])
+    assert occupied > 1_000_000, occupied
+    assert np.array_equal(grid_gpu, grid_ref), f"{np.count_nonzero(grid_gpu != grid_ref)} cells differ"
+    o.close()
+    g.close()
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_config_twenty_substeps_bit_exact(gpu, oracle_mod, name):
+    spec = SCENES[name](gpu)
+    g = GpuScene(gpu, spec)
+    assert g.step(20) == 0
+    got = g.particles()
+    o, want = _oracle(oracle_mod, spec, 20)
+    compare_states(got, want)
+    o.close()
+    g.close()
+
+
+def test_config0_hundred_substeps_against_fp64(gpu, oracle_mod):
+    """Config 0 as specified (100 substeps): bit-exact against the f32 oracle,
+    and each aggregate within 1e-3 of the f64 oracle."""
+    spec = _c0(gpu)
+    g = GpuScene(gpu, spec)
+    assert g.step(100) == 0
+    got = g.particles()
+    g.close()
+    o, want = _oracle(oracle_mod, spec, 100)
+    o.close()
+    compare_states(got, want)
+    o, w64 = _oracle(oracle_mod, spec, 100, fp64=True)
+    o.close()
+    err = _agg_errors(got, w64)
+    assert all(v <= AGG_TOL for v in err.values()), err
+
+
+def test_config1_aggregates_against_fp64(gpu, oracle_mod):
+    """Config 1 (two spheres colliding, PBMPM x6, box + icosphere collider),
+    20 substeps: aggregates within 1e-3 of the f64 oracle."""
+    spec = _c1(gpu)
+    g = GpuScene(gpu, spec)
+    assert g.step(20) == 0
+    got = g.particles()
+    g.close()
+    o, w64 = _oracle(oracle_mod, spec, 20, fp64=True)
+    o.close()
+    err = _agg_errors(got, w64)
+    assert all(v <= AGG_TOL for v in err.values()), err
+
+
+def test_config2_full_size_substep_bit_exact(gpu, oracle_mod):
+    """One substep of the full 4,194,304-particle slab (the benchmark
+    workload) against the f32 oracle, every particle field bit for bit."""
+    spec = gpu.scenes.c2_large_pbmpm()
+    assert spec.particles.shape[0] == 4_194_304
+    g = GpuScene(gpu, spec)
+    assert g.step(1) == 0
+    got = g.particles()
+    g.close()
+    o, want = _oracle(oracle_mod, spec, 1)
+    o.close()
+    compare_states(got, want)
+
+
+def test_config3_batch_scenes_against_oracle(gpu, oracle_mod):
+    """A small batch of config-3 scenes (explicit, each with its own E,
+    theta_c and dx) in one handle: each scene equals the f32 oracle's run of
+    that scene alone, bit for bit."""
+    specs = gpu.scenes.c3_batched(n_scenes=5, seed=8, lo_count=500, hi_count=6000)
+    for s in specs:
+        _config_mode(s)
+    b = gpu.GpuMpmBatch(specs)
+    b.step(gpu.GpuSimulationMethodType.ExplicitMpm, 5)
+    assert b.mpm.sync() == 0
+    rec = b.mpm.read_particles()
+    for i, spec in enumerate(specs):
+        o, want = _oracle(oracle_mod, spec, 5)
+        o.close()
+        compare_states(b.scene_particles(i, rec), want)
+    b.close()

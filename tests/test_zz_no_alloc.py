@@ -87,3 +87,60 @@ def test_noalloc_rejects_more_particles_than_its_limit(gpu):
                               0, None, 0, None, err, len(err))
     assert rc == -3, rc  # MPM_ERR_CAPACITY, before any device work
     assert b"65536" in err.value
+
+
+def test_noalloc_reports_tile_overflow(gpu):
+    """More occupied 8^3-cell tiles than the array holds (512): the call
+    returns MPM_ERR_DEVICE_STATUS with status bit 0x2 (a status the host
+    reads; nothing faults), and the scratch array is left usable: a normal
+    call right after it matches the handle step again."""
+    import torch
+
+    lib = gpu.load()
+    spec = gpu.scenes.parity_scene(kind="explicit", n_side=13, res=256)
+    rng = np.random.default_rng(17)
+    n = spec.particles.shape[0]
+    spec.particles["pos"] = rng.uniform(0.05, 0.95, size=(n, 3)).astype(np.float32)
+    params = make_params(gpu, spec.params)
+    ub = spec.uniforms.bytes()
+    dev = _device_copy(torch, spec.particles)
+    status = C.c_uint32(0)
+    err = C.create_string_buffer(256)
+    rc = lib.mpm_step_noalloc(0, C.c_void_p(torch.cuda.current_stream().cuda_stream), C.c_void_p(dev.data_ptr()), n,
+                              0, ub, len(ub), C.byref(params), None, 0, 0, None, 0, C.byref(status), err, len(err))
+    assert rc == -5, (rc, err.value)  # MPM_ERR_DEVICE_STATUS
+    assert status.value & 0x2, status.value
+    assert b"512" in err.value
+    # the next call starts from a clean array
+    spec2 = gpu.scenes.parity_scene(kind="explicit", n_side=12)
+    g = GpuScene(gpu, spec2)
+    assert g.step(1) == 0
+    want = g.particles()
+    g.close()
+    dev2 = _device_copy(torch, spec2.particles)
+    _noalloc_step(lib, spec2, make_params(gpu, spec2.params), dev2, spec2.particles.shape[0], None)
+    torch.cuda.synchronize()
+    compare_states(dev2.cpu().numpy().view(spec2.particles.dtype), want)
+
+
+def test_noalloc_without_status_does_not_wait(gpu):
+    """With status_out NULL the call only enqueues work; after the caller
+    synchronises, the records equal the handle step's."""
+    import torch
+
+    lib = gpu.load()
+    spec = gpu.scenes.parity_scene(kind="pbmpm", n_side=12, with_collider=False)
+    n = spec.particles.shape[0]
+    g = GpuScene(gpu, spec)
+    assert g.step(1) == 0
+    want = g.particles()
+    g.close()
+    params = make_params(gpu, spec.params)
+    ub = spec.uniforms.bytes()
+    dev = _device_copy(torch, spec.particles)
+    err = C.create_string_buffer(256)
+    rc = lib.mpm_step_noalloc(0, C.c_void_p(torch.cuda.current_stream().cuda_stream), C.c_void_p(dev.data_ptr()), n,
+                              spec.method, ub, len(ub), C.byref(params), None, 0, 0, None, 0, None, err, len(err))
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    compare_states(dev.cpu().numpy().view(spec.particles.dtype), want)

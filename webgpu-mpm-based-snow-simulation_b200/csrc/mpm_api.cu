@@ -1574,6 +1574,13 @@ int na_fail(char* err, size_t err_len, int code, const char* fmt, ...) {
 
 }  // namespace
 
+// Writes the call's scene record and particle range into the scratch array.
+__global__ void k_na_store_scene(SceneDev sc, uint32_t n_particles, SceneDev* scene, uint32_t* scene_first) {
+    *scene = sc;
+    scene_first[0] = 0u;
+    scene_first[1] = n_particles;
+}
+
 // The scratch itself.  A host-side use of this name refers to a host stand-in,
 // not to device memory: host code passes kernels the address returned by
 // cudaGetSymbolAddress for the current device instead.
@@ -1649,7 +1656,6 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
         return na_fail(err, err_len, MPM_ERR_ARG, "fixedPointScale and timestep must be > 0");
     if (sc.dev.res[0] <= 0 || sc.dev.res[1] <= 0 || sc.dev.res[2] <= 0)
         return na_fail(err, err_len, MPM_ERR_ARG, "grid resolution must be > 0");
-    const uint32_t scene_first[2] = {0u, n_particles};
 
     unsigned char* b = D.base;
     Ctx c{};
@@ -1693,8 +1699,11 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     NA_CK(cudaMemsetAsync(c.keys, 0xff, NA_H * 8, s));
     NA_CK(cudaMemsetAsync(c.slot_count, 0, NA_H * 4, s));
     NA_CK(cudaMemsetAsync(c.counters, 0, sizeof(Counters), s));
-    NA_CK(cudaMemcpyAsync((void*)c.scenes, &sc.dev, sizeof(SceneDev), cudaMemcpyHostToDevice, s));
-    NA_CK(cudaMemcpyAsync((void*)c.scene_first, scene_first, sizeof(scene_first), cudaMemcpyHostToDevice, s));
+    // the scene record reaches the device as a kernel argument (copied at
+    // launch), so no host buffer has to outlive the call and the host does
+    // not wait for the stream here
+    k_na_store_scene<<<1, 1, 0, s>>>(sc.dev, n_particles, (SceneDev*)c.scenes, (uint32_t*)c.scene_first);
+    NA_CK(cudaGetLastError());
     k_iota<<<(n_particles + 255u) / 256u, 256, 0, s>>>((uint32_t*)c.order_in, n_particles);
     NA_CK(cudaGetLastError());
     auto run = [&](uint32_t kid) {
