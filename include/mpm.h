@@ -376,7 +376,7 @@ int mpm_get_plasticity_stats(MpmHandle* h, MpmPlasticityStats* out, int reset);
 #define MPM_NOALLOC_MAX_TILES 512u
 #define MPM_NOALLOC_TILE_EDGE 8u
 #define MPM_NOALLOC_HASH_SLOTS 8192u
-#define MPM_NOALLOC_SCRATCH_BYTES (25u << 20)
+#define MPM_NOALLOC_SCRATCH_BYTES (50u << 20)
 int mpm_step_noalloc(int device, void* stream, void* particles, uint32_t n_particles, int method,
                      const void* uniforms, size_t uniform_bytes, const MpmParams* params,
                      const uint32_t* collider_data, size_t collider_words, uint32_t num_indices,

@@ -13,10 +13,30 @@
  * max(byte / 127, -1).  The triangulation table is an input (the caller's),
  * and the output order is: active 8^3 blocks ascending, cells in block order
  * (x fastest), triangles in table order, 6 floats per vertex.
+ *
+ * or_mc_tables returns the reference's case table (MC_TRI_TABLE of
+ * marchingCubes/triTable.wgsl and MC_TRI_COUNTS of prelude.wgsl, a data
+ * contract, shared with the CUDA passes through mpm_mc_table.h) and its edge
+ * endpoints (MC_EDGE_V0 / MC_EDGE_V1, prelude.wgsl:45-46).
  */
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+
+#include "../webgpu-mpm-based-snow-simulation_b200/csrc/mpm_mc_table.h"
+
+/* prelude.wgsl:45-46: edge e joins cube vertices EV0[e] and EV1[e] */
+static const uint8_t EV0[12] = {0, 4, 2, 6, 0, 1, 2, 3, 0, 1, 4, 5};
+static const uint8_t EV1[12] = {1, 5, 3, 7, 4, 5, 6, 7, 2, 3, 6, 7};
+
+void or_mc_tables(int8_t* tri, uint8_t* count, uint8_t* ev) {
+    memcpy(tri, MPM_MC_TRI_TABLE, sizeof(MPM_MC_TRI_TABLE));
+    memcpy(count, MPM_MC_TRI_COUNTS, sizeof(MPM_MC_TRI_COUNTS));
+    for (int e = 0; e < 12; e++) {
+        ev[2 * e] = EV0[e];
+        ev[2 * e + 1] = EV1[e];
+    }
+}
 
 #define MC_ISO 0.15f
 

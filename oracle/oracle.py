@@ -24,6 +24,7 @@ UNIFORMS_BYTES = 37376
 def build(force: bool = False) -> str:
     srcs = [os.path.join(HERE, f) for f in ("mpm_oracle.c", "mpm_oracle.h", "bvh_oracle.c", "mlp_oracle.c", "splat_oracle.c",
                                              "scatter_oracle.c", "raymarch_oracle.c", "mc_oracle.c", "Makefile")]
+    srcs.append(os.path.join(HERE, "..", "webgpu-mpm-based-snow-simulation_b200", "csrc", "mpm_mc_table.h"))
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     return LIB
@@ -80,6 +81,7 @@ def lib():
             "or_scatter": (None, [V, U32, V, V, U32, V]),
             "or_raymarch": (None, [V, V, V, V, C.c_float, V, U32, U32, U32, V, V, V]),
             "or_marching_cubes": (None, [V, V, V, V, V, C.c_float, V, V, V, V, U32, V]),
+            "or_mc_tables": (None, [V, V, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -290,69 +292,15 @@ def raymarch(mass_grid, grid_min, grid_max, scale, inv_view_proj, time, width, h
 
 # ---- marching cubes (mc_oracle.c) and its triangulation table -----------
 def mc_tables():
-    """Triangulation table by contour tracing on the cube: the reference's
-    numbering (vertex id = x + 2 z + 4 y; edges along x, then y, then z, each
-    group ordered by the other two coordinates, first + 2 second); on every
-    face, walking its corners counter-clockwise seen from outside, each crossing
-    from inside to outside is joined to the crossing that opened its run of
-    inside corners (inside corners kept apart on ambiguous faces); the joined
-    crossings form loops, each fanned from its first edge.  Returns (tri int8
-    [256, 16] padded with -1, counts uint8 [256], edge endpoints uint8 [12, 2])."""
-    import math
-
-    def pos(v):
-        return (v & 1, (v >> 2) & 1, (v >> 1) & 1)
-
-    edges = []
-    for a in range(3):
-        o = [k for k in range(3) if k != a]
-        for q in range(4):
-            p0 = [0, 0, 0]
-            p0[o[0]], p0[o[1]] = q & 1, q >> 1
-            p1 = list(p0)
-            p1[a] = 1
-            edges.append((p0[0] + 2 * p0[2] + 4 * p0[1], p1[0] + 2 * p1[2] + 4 * p1[1]))
-    lookup = {frozenset(e): i for i, e in enumerate(edges)}
-    faces = []
-    for a in range(3):
-        for side in (0, 1):
-            b, c = (a + 1) % 3, (a + 2) % 3
-            u, w = (b, c) if side else (c, b)
-            cs = sorted((v for v in range(8) if pos(v)[a] == side),
-                        key=lambda v: math.atan2(pos(v)[w] - 0.5, pos(v)[u] - 0.5))
-            faces.append(cs)
-    tri = np.full((256, 16), -1, np.int8)
+    """The reference's marching-cubes case table (marchingCubes/triTable.wgsl,
+    prelude.wgsl MC_TRI_COUNTS) and edge endpoints (prelude.wgsl:45-46), from
+    mc_oracle.c.  Returns (tri int8 [256, 16] padded with -1, counts uint8
+    [256], edge endpoints uint8 [12, 2])."""
+    tri = np.zeros((256, 16), np.int8)
     cnt = np.zeros(256, np.uint8)
-    for case in range(256):
-        inside = [(case >> v) & 1 for v in range(8)]
-        nxt = {}
-        for cc in faces:
-            kinds, ids = [], []
-            for i in range(4):
-                a, b = cc[i], cc[(i + 1) % 4]
-                ids.append(lookup[frozenset((a, b))])
-                kinds.append(1 if inside[a] and not inside[b] else (-1 if inside[b] and not inside[a] else 0))
-            for i in range(4):
-                if kinds[i] == 1:
-                    j = (i + 3) % 4
-                    while kinds[j] != -1:
-                        j = (j + 3) % 4
-                    nxt[ids[i]] = ids[j]
-        out, seen = [], set()
-        for e in range(12):
-            if e in nxt and e not in seen:
-                loop = [e]
-                seen.add(e)
-                x = nxt[e]
-                while x != e:
-                    loop.append(x)
-                    seen.add(x)
-                    x = nxt[x]
-                for t in range(1, len(loop) - 1):
-                    out += [loop[0], loop[t], loop[t + 1]]
-        cnt[case] = len(out) // 3
-        tri[case, :len(out)] = out
-    return tri, cnt, np.array(edges, np.uint8)
+    ev = np.zeros((12, 2), np.uint8)
+    lib().or_mc_tables(tri.ctypes.data, cnt.ctypes.data, ev.ctypes.data)
+    return tri, cnt, ev
 
 
 def marching_cubes(density, grid_min, grid_max, scale, mc_res, tables=None, max_vertices=None):

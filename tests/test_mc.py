@@ -1,9 +1,10 @@
 """Marching cubes (mcListBlocks, mcVertexDensity, mcGenerate): the library's
-triangulation table equals the oracle's independent generator and gives
-closed, consistently oriented meshes on the CPU; the CUDA passes equal the
-oracle's restatement vertex for vertex on the GPU, on a synthetic density
-field with partial blocks, with a vertex cap, and through the chain
-simulation -> calculateDensity -> mesh."""
+case table is the reference's (the oracle reads the same table and restates
+the reference's edge endpoints), consistent with the reference's separate
+per-case triangle counts; the CUDA passes equal the oracle's restatement
+vertex for vertex on the GPU, on a synthetic density field with partial
+blocks, with a vertex cap, and through the chain simulation ->
+calculateDensity -> mesh."""
 from collections import Counter
 
 import numpy as np
@@ -25,20 +26,27 @@ def _blobs(res, seed=0, scale=2.0 ** 28):
     return np.floor(g * 0.6 * scale).astype(np.uint32)
 
 
-def test_tables_match_oracle_generator(pkg, oracle_mod):
+def test_tables_are_the_reference_table(pkg, oracle_mod):
     tri, cnt, ev = pkg.pipeline.mc_tables()
     otri, ocnt, oev = oracle_mod.mc_tables()
-    assert np.array_equal(tri, otri) and np.array_equal(cnt, ocnt) and np.array_equal(ev, oev)
+    assert np.array_equal(tri, otri) and np.array_equal(cnt, ocnt)
+    # the library derives the edge endpoints from the numbering; the oracle
+    # restates the reference's MC_EDGE_V0 / MC_EDGE_V1
+    assert np.array_equal(ev, oev)
     assert cnt[0] == 0 and cnt[255] == 0 and cnt.max() <= 5
-    # edge numbering: along x, then y, then z (vertex id = x + 2z + 4y)
-    assert ev[0].tolist() == [0, 1] and ev[4].tolist() == [0, 4] and ev[8].tolist() == [0, 2]
+    # first cases of MC_TRI_TABLE (triTable.wgsl:6-9)
+    assert tri[1][:3].tolist() == [0, 8, 4] and tri[2][:3].tolist() == [0, 5, 9]
+    assert tri[3][:6].tolist() == [8, 4, 9, 9, 4, 5]
     for c in range(256):
+        # the reference's per-case counts (MC_TRI_COUNTS) equal its triangle lists
         used = tri[c][: 3 * cnt[c]]
-        assert np.all(tri[c][3 * cnt[c]:] == -1)
+        assert np.all(used >= 0) and np.all(tri[c][3 * cnt[c]:] == -1)
         # every triangle edge index is a cut edge of the case
         for e in used:
             a, b = ev[e]
             assert ((c >> a) & 1) != ((c >> b) & 1)
+    # the total number of triangles over all cases
+    assert int(cnt.sum()) == int((tri >= 0).sum()) // 3
 
 
 def test_oracle_mesh_is_closed_and_oriented(oracle_mod):

@@ -188,3 +188,72 @@ def test_permutation_invariance(gpu):
     g.close()
     inv = np.argsort(perm)
     compare_states(b[inv], a)
+
+
+def test_bound_device_buffer_updated_after_each_step(gpu, oracle_mod):
+    """Zero-copy binding (mpm_bind_particles_device): the library advances
+    its own tile-ordered copy of the state and writes the caller's buffer
+    back, in the caller's order, at the end of every step call."""
+    import torch
+
+    spec = _scene(gpu, kind="pbmpm", with_collider=True)
+    n = spec.particles.shape[0]
+    dev = torch.from_numpy(spec.particles.view(np.uint8).reshape(-1).copy()).cuda()
+    g = GpuScene(gpu, spec)
+    g.buf.bind_particles_device(dev.data_ptr(), n)
+    for steps in (1, 3):
+        assert g.step(1 if steps == 1 else 2) == 0
+        torch.cuda.synchronize()
+        got = dev.cpu().numpy().view(spec.particles.dtype)
+        _, want = run_oracle(oracle_mod, spec, n_steps=steps)
+        compare_states(got, want)
+    g.close()
+
+
+def test_reading_between_steps_changes_nothing(gpu):
+    """Reading the records (which brings the caller-order copy up to date)
+    between substeps leaves the state the substeps advance untouched."""
+    spec = _scene(gpu, kind="explicit", with_collider=True)
+    a = GpuScene(gpu, spec)
+    assert a.step(4) == 0
+    want = a.particles()
+    a.close()
+    b = GpuScene(gpu, spec)
+    for _ in range(4):
+        assert b.step(1) == 0
+        b.particles()
+    compare_states(b.particles(), want)
+    b.close()
+
+
+def test_device_upload_and_pointer(gpu, oracle_mod):
+    """Records uploaded from device memory, read back into device memory,
+    and the device pointer the library hands out: all hold the current
+    records in the caller's order."""
+    import ctypes as C
+
+    import torch
+
+    spec = _scene(gpu, kind="explicit", n_side=10)
+    n = spec.particles.shape[0]
+    nbytes = n * spec.particles.dtype.itemsize
+    src = torch.from_numpy(spec.particles.view(np.uint8).reshape(-1).copy()).cuda()
+    g = GpuScene(gpu, spec)
+    g.buf.write_particles_device(src.data_ptr(), n)
+    assert g.step(2) == 0
+    _, want = run_oracle(oracle_mod, spec, n_steps=2)
+    out = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    lib = gpu.load()
+    assert lib.mpm_get_particles(g.buf.handle, C.c_void_p(out.data_ptr()), n, 1) == 0
+    torch.cuda.synchronize()
+    compare_states(out.cpu().numpy().view(spec.particles.dtype), want)
+    ptr = lib.mpm_particles_device_ptr(g.buf.handle)
+    assert ptr
+    assert g.buf.sync() == 0
+
+    class _Raw:  # a view of the library's record buffer for torch
+        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, True), "version": 3}
+
+    recs = torch.as_tensor(_Raw(), device="cuda").clone()
+    compare_states(recs.cpu().numpy().view(spec.particles.dtype), want)
+    g.close()

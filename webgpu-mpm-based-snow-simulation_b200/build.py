@@ -14,7 +14,7 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG_DIR, "csrc")
 LIB_PATH = os.path.join(PKG_DIR, "libmpm.so")
 SOURCES = ["mpm_kernels.cu", "mpm_mlp.cu", "mpm_splat.cu", "mpm_scatter.cu", "mpm_raymarch.cu", "mpm_mc.cu", "mpm_api.cu", "bvh_build.cpp", "bvh_gpu.cu"]
-HEADERS = ["mpm_math.cuh", "mpm_pow_tables.h", "mpm_engine.cuh", "mpm_plast.cuh", "mpm_tc.cuh", "mpm_mlp.cuh",
+HEADERS = ["mpm_math.cuh", "mpm_pow_tables.h", "mpm_mc_table.h", "mpm_engine.cuh", "mpm_plast.cuh", "mpm_tc.cuh", "mpm_mlp.cuh",
            os.path.join("..", "..", "include", "mpm.h")]
 
 NVCC_FLAGS = [

@@ -106,12 +106,17 @@ struct MpmHandle {
     bool auto_tiles = true;   // tile capacity sized from the first binning, grown at sync points
     bool auto_cap = true;     // hash capacity grown at sync points
 
-    float4* particles = nullptr;
+    float4* particles = nullptr;      // the reference records in the caller's order (the boundary)
     bool own_particles = true;
     uint32_t n_particles = 0;
-    uint32_t* order[2] = {nullptr, nullptr};
-    int order_parity = 0;
-    bool order_valid = false;
+    // the state the substeps advance: REC_PLANES planes per buffer, slots in
+    // tile order; work[work_cur] is current once work_valid
+    float4* work[2] = {nullptr, nullptr};
+    uint32_t* ids[2] = {nullptr, nullptr};   // caller index of each work slot
+    uint32_t* sorted = nullptr;
+    int work_cur = 0;
+    bool work_valid = false;       // false: `particles` holds the state (just set, bound or scattered)
+    bool records_stale = false;    // `particles` is older than work[work_cur]
     uint32_t* bin_slot = nullptr;
     uint32_t* bin_rank = nullptr;
     unsigned long long* keys = nullptr;
@@ -352,7 +357,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     destroy_graphs(h);
     for (auto& t : h->pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     for (auto e : h->event_pool) cudaEventDestroy(e);
-    void* bufs[] = {h->order[0], h->order[1], h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
+    void* bufs[] = {h->work[0], h->work[1], h->ids[0], h->ids[1], h->sorted, h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
                     h->tiles[0], h->tiles[1], h->tiles[2], h->tile_rm, h->d_scenes, h->d_scene_first, h->counters,
                     h->iter_rec, h->st_nbr, h->tile_order,
@@ -447,8 +452,11 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
         h->own_stream = true;
     }
     CK(h, cudaMalloc(&h->particles, (size_t)N * MPM_PARTICLE_BYTES));
-    CK(h, cudaMalloc(&h->order[0], (size_t)N * 4));
-    CK(h, cudaMalloc(&h->order[1], (size_t)N * 4));
+    for (int i = 0; i < 2; i++) {
+        CK(h, cudaMalloc(&h->work[i], (size_t)N * MPM_PARTICLE_BYTES));
+        CK(h, cudaMalloc(&h->ids[i], (size_t)N * 4));
+    }
+    CK(h, cudaMalloc(&h->sorted, (size_t)N * 4));
     CK(h, cudaMalloc(&h->bin_slot, (size_t)N * 4));
     CK(h, cudaMalloc(&h->bin_rank, (size_t)N * 4));
     CK(h, cudaMalloc(&h->iter_rec, (size_t)N * IR_PLANES * sizeof(float4)));
@@ -543,7 +551,7 @@ extern "C" int mpm_set_scene_range(MpmHandle* h, uint32_t scene, uint32_t first,
 static int set_count(MpmHandle* h, uint32_t n) {
     if (n != h->n_particles) {
         h->n_particles = n;
-        h->order_valid = false;
+        h->work_valid = false;
         destroy_graphs(h);
         if (h->n_scenes == 1) {
             h->scenes[0].dev.p_first = 0;
@@ -551,6 +559,44 @@ static int set_count(MpmHandle* h, uint32_t n) {
             h->scenes_dirty = true;
         }
     }
+    return MPM_OK;
+}
+
+// Caller records -> work planes (slot t = caller index t).  One thread per
+// record word: a warp reads 512 contiguous bytes of records and writes two or
+// three runs of each plane.
+__global__ void k_work_load(const float4* rec, uint32_t n, float4* work, uint32_t* ids) {
+    const size_t total = (size_t)n * REC_PLANES;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t t = (uint32_t)(i / REC_PLANES), q = (uint32_t)(i % REC_PLANES);
+        work[(size_t)q * n + t] = rec[i];
+        if (q == 0u) ids[t] = t;
+    }
+}
+
+// Work planes -> caller records: word q of slot t goes to record ids[t]
+// (consecutive threads write the consecutive words of one record).
+__global__ void k_work_store(const float4* work, const uint32_t* ids, uint32_t n, float4* rec) {
+    const size_t total = (size_t)n * REC_PLANES;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t t = (uint32_t)(i / REC_PLANES), q = (uint32_t)(i % REC_PLANES);
+        rec[(size_t)__ldg(ids + t) * REC_PLANES + q] = work[(size_t)q * n + t];
+    }
+}
+
+static unsigned work_grid(uint32_t n) {
+    size_t blocks = ((size_t)n * REC_PLANES + 255u) / 256u;
+    return (unsigned)std::max<size_t>(1, std::min<size_t>(blocks, 148u * 16u));
+}
+
+// Brings the caller-order records up to date with the work state (enqueued on
+// the handle's stream): called before anything reads `particles`.
+static int flush_records(MpmHandle* h) {
+    if (!h->records_stale || !h->work_valid || h->n_particles == 0) return MPM_OK;
+    k_work_store<<<work_grid(h->n_particles), 256, 0, h->stream>>>(h->work[h->work_cur], h->ids[h->work_cur],
+                                                                   h->n_particles, h->particles);
+    CK(h, cudaGetLastError());
+    h->records_stale = false;
     return MPM_OK;
 }
 
@@ -562,7 +608,8 @@ extern "C" int mpm_set_particles(MpmHandle* h, const void* src, uint32_t n, int 
     if (n) CK(h, cudaMemcpyAsync(h->particles, src, (size_t)n * MPM_PARTICLE_BYTES,
                                  src_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
     set_count(h, n);
-    h->order_valid = false;
+    h->work_valid = false;
+    h->records_stale = false;
     return MPM_OK;
 }
 
@@ -570,6 +617,8 @@ extern "C" int mpm_get_particles(MpmHandle* h, void* dst, uint32_t n, int dst_is
     if (!h || (!dst && n)) return MPM_ERR_ARG;
     if (n > h->n_particles) return fail(h, MPM_ERR_ARG, "asked for %u particles, have %u", n, h->n_particles);
     cudaSetDevice(h->device);
+    int r = flush_records(h);
+    if (r) return r;
     if (n) CK(h, cudaMemcpyAsync(dst, h->particles, (size_t)n * MPM_PARTICLE_BYTES,
                                  dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
     if (!dst_is_device) CK(h, cudaStreamSynchronize(h->stream));
@@ -586,11 +635,17 @@ extern "C" int mpm_bind_particles_device(MpmHandle* h, void* dptr, uint32_t n) {
     h->own_particles = false;
     destroy_graphs(h);
     set_count(h, n);
-    h->order_valid = false;
+    h->work_valid = false;
+    h->records_stale = false;
     return MPM_OK;
 }
 
-extern "C" void* mpm_particles_device_ptr(MpmHandle* h) { return h ? (void*)h->particles : nullptr; }
+extern "C" void* mpm_particles_device_ptr(MpmHandle* h) {
+    if (!h) return nullptr;
+    cudaSetDevice(h->device);
+    if (flush_records(h)) return nullptr;
+    return (void*)h->particles;
+}
 
 extern "C" int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* data, size_t words, uint32_t num_indices,
                                 const void* nodes, uint32_t n_nodes) {
@@ -711,11 +766,13 @@ __global__ void k_iota(uint32_t* o, uint32_t n) {
     if (i < n) o[i] = i;
 }
 
-static Ctx make_ctx(MpmHandle* h, int parity) {
+static Ctx make_ctx(MpmHandle* h, int cur) {
     Ctx c{};
-    c.particles = h->particles;
-    c.order_in = h->order[parity];
-    c.sorted = h->order[parity ^ 1];
+    c.work_in = h->work[cur];
+    c.work_out = h->work[cur ^ 1];
+    c.ids_in = h->ids[cur];
+    c.ids_out = h->ids[cur ^ 1];
+    c.sorted = h->sorted;
     c.bin_slot = h->bin_slot;
     c.bin_rank = h->bin_rank;
     c.keys = h->keys;
@@ -876,7 +933,7 @@ static uint32_t tiles_for(uint32_t n_st) { return std::max(1024u, n_st + n_st / 
 // per occupied tile, the tile buffers to 1.5x the occupied tiles.
 static int size_from_binning(MpmHandle* h) {
     for (int attempt = 0; attempt < 4; attempt++) {
-        Ctx c = make_ctx(h, h->order_parity);
+        Ctx c = make_ctx(h, h->work_cur);
         c.max_tiles = 0xFFFFFFFFu;  // no tile storage is touched by this pass
         for (uint32_t k : {K_CLEAR_TABLE, K_BIN_INSERT, K_COMPACT_A, K_COMPACT_B, K_COMPACT_C}) {
             cudaError_t e = launch_e(h->tile_edge, k, c, h->stream, h->n_sms, 0, 0, nullptr);
@@ -909,22 +966,17 @@ static int prepare_step(MpmHandle* h) {
     cudaSetDevice(h->device);
     int r = upload_scenes(h);
     if (r) return r;
+    if (!h->work_valid) {
+        // the caller's records become the work state, slot t = particle t
+        k_work_load<<<work_grid(h->n_particles), 256, 0, h->stream>>>(h->particles, h->n_particles,
+                                                                      h->work[h->work_cur], h->ids[h->work_cur]);
+        CK(h, cudaGetLastError());
+        h->work_valid = true;
+        h->records_stale = false;
+    }
     if (h->tiles[0] == nullptr) {
-        if (!h->order_valid) {
-            k_iota<<<(h->n_particles + 255) / 256, 256, 0, h->stream>>>(h->order[h->order_parity], h->n_particles);
-            CK(h, cudaGetLastError());
-        }
         r = size_from_binning(h);
         if (r) return r;
-    }
-    if (!h->order_valid) {
-        // both order buffers start as the identity so every entry the next
-        // binning pass reads is a valid particle index
-        k_iota<<<(h->n_particles + 255) / 256, 256, 0, h->stream>>>(h->order[0], h->n_particles);
-        CK(h, cudaGetLastError());
-        k_iota<<<(h->n_particles + 255) / 256, 256, 0, h->stream>>>(h->order[1], h->n_particles);
-        CK(h, cudaGetLastError());
-        h->order_valid = true;
     }
     return MPM_OK;
 }
@@ -933,7 +985,7 @@ static uint64_t graph_signature(MpmHandle* h) {
     uint64_t s = h->n_particles;
     s = s * 1315423911ull + h->n_scenes;
     s = s * 1315423911ull + h->scenes[0].params.n_iter;
-    s = s * 1315423911ull + (uint64_t)(uintptr_t)h->particles;
+    s = s * 1315423911ull + (uint64_t)(uintptr_t)h->work[0];
     s = s * 1315423911ull + (uint64_t)h->plast_mode;
     s = s * 1315423911ull + (uint64_t)(uintptr_t)(h->mlp ? h->mlp->params : nullptr);
     s = s * 1315423911ull + (uint64_t)(uintptr_t)h->pair_x + h->pair_cap;
@@ -944,7 +996,7 @@ static uint64_t graph_signature(MpmHandle* h) {
 }
 
 static int run_substep(MpmHandle* h, int method) {
-    int par = h->order_parity;
+    int par = h->work_cur;
     if (h->use_graphs && !h->timing) {
         uint64_t sig = graph_signature(h);
         if (!h->graph[method][par] || h->graph_sig[method][par] != sig) {
@@ -969,7 +1021,8 @@ static int run_substep(MpmHandle* h, int method) {
         cudaError_t e = enqueue_substep(h, method, par, false, false);
         if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
     }
-    h->order_parity ^= 1;
+    h->work_cur ^= 1;
+    h->records_stale = true;
     return MPM_OK;
 }
 
@@ -982,6 +1035,10 @@ extern "C" int mpm_step(MpmHandle* h, int method, uint32_t n_substeps) {
         r = run_substep(h, method);
         if (r) return r;
     }
+    // a caller-bound buffer is the caller's view of the state: bring it up to
+    // date after every call (library-owned records are brought up to date
+    // when read)
+    if (!h->own_particles) return flush_records(h);
     return MPM_OK;
 }
 
@@ -1002,9 +1059,9 @@ extern "C" int mpm_step_p2g_only(MpmHandle* h, int method) {
     if (method != MPM_METHOD_EXPLICIT && method != MPM_METHOD_PBMPM) return fail(h, MPM_ERR_ARG, "bad method %d", method);
     int r = prepare_step(h);
     if (r) return r;
-    cudaError_t e = enqueue_substep(h, method, h->order_parity, false, true);
+    // the first transfer only: the grid is formed, the particle state is not advanced
+    cudaError_t e = enqueue_substep(h, method, h->work_cur, false, true);
     if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
-    h->order_parity ^= 1;
     return MPM_OK;
 }
 
@@ -1077,7 +1134,7 @@ extern "C" int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_u
     int4* dout = nullptr;
     CK(h, cudaMalloc(&dout, need * 16));
     CK(h, cudaMemsetAsync(dout, 0, need * 16, h->stream));
-    Ctx c = make_ctx(h, h->order_parity);
+    Ctx c = make_ctx(h, h->work_cur);
     c.tiles_b = h->tiles[h->last_tiles];
     // the PBMPM iterations write momentum only: the mass sums are the first transfer's
     c.tiles_m = h->last_tiles != 0 ? h->tiles[0] : nullptr;
@@ -1099,6 +1156,8 @@ static int splat(MpmHandle* h, uint32_t scene, int kind, const uint32_t* res, ui
     if (!out_dev) return fail(h, MPM_ERR_ARG, "null output buffer");
     cudaSetDevice(h->device);
     r = upload_scenes(h);
+    if (r) return r;
+    r = flush_records(h);
     if (r) return r;
     const SceneDev& d = h->scenes[scene].dev;
     SplatArgs a{};
@@ -1221,7 +1280,8 @@ extern "C" int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(dv);
     if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "scatter: %s", cudaGetErrorString(e));
-    h->order_valid = false;
+    h->work_valid = false;
+    h->records_stale = false;
     return MPM_OK;
 }
 
@@ -1525,8 +1585,11 @@ static_assert(MPM_NOALLOC_TILE_EDGE == NA_EDGE, "header and engine disagree on t
 
 constexpr size_t na_round(size_t v) { return (v + 255u) & ~(size_t)255u; }
 constexpr size_t NA_P = MPM_NOALLOC_MAX_PARTICLES, NA_H = MPM_NOALLOC_HASH_SLOTS;
-constexpr size_t NA_ORDER = 0;                                          // particle ids, input order
-constexpr size_t NA_SORTED = NA_ORDER + na_round(NA_P * 4);             // particle ids grouped by tile
+constexpr size_t NA_WORK0 = 0;                                          // particle state in, planes
+constexpr size_t NA_WORK1 = NA_WORK0 + na_round(NA_P * MPM_PARTICLE_BYTES);   // particle state out, tile order
+constexpr size_t NA_IDS0 = NA_WORK1 + na_round(NA_P * MPM_PARTICLE_BYTES);    // caller index per slot
+constexpr size_t NA_IDS1 = NA_IDS0 + na_round(NA_P * 4);
+constexpr size_t NA_SORTED = NA_IDS1 + na_round(NA_P * 4);              // input slots grouped by tile
 constexpr size_t NA_BIN_SLOT = NA_SORTED + na_round(NA_P * 4);
 constexpr size_t NA_BIN_RANK = NA_BIN_SLOT + na_round(NA_P * 4);
 constexpr size_t NA_KEYS = NA_BIN_RANK + na_round(NA_P * 4);            // tile hash keys (u64)
@@ -1659,8 +1722,10 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
 
     unsigned char* b = D.base;
     Ctx c{};
-    c.particles = (float4*)particles;
-    c.order_in = (const uint32_t*)(b + NA_ORDER);
+    c.work_in = (const float4*)(b + NA_WORK0);
+    c.work_out = (float4*)(b + NA_WORK1);
+    c.ids_in = (const uint32_t*)(b + NA_IDS0);
+    c.ids_out = (uint32_t*)(b + NA_IDS1);
     c.sorted = (uint32_t*)(b + NA_SORTED);
     c.bin_slot = (uint32_t*)(b + NA_BIN_SLOT);
     c.bin_rank = (uint32_t*)(b + NA_BIN_RANK);
@@ -1704,7 +1769,9 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     // not wait for the stream here
     k_na_store_scene<<<1, 1, 0, s>>>(sc.dev, n_particles, (SceneDev*)c.scenes, (uint32_t*)c.scene_first);
     NA_CK(cudaGetLastError());
-    k_iota<<<(n_particles + 255u) / 256u, 256, 0, s>>>((uint32_t*)c.order_in, n_particles);
+    // the caller's records become the input state (slot t = particle t)
+    k_work_load<<<work_grid(n_particles), 256, 0, s>>>((const float4*)particles, n_particles, (float4*)c.work_in,
+                                                       (uint32_t*)c.ids_in);
     NA_CK(cudaGetLastError());
     auto run = [&](uint32_t kid) {
         int grid = std::max(1, D.n_sms * std::max(1, D.blocks_per_sm[kid]));
@@ -1729,6 +1796,9 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
         c.g2p_rm = params->n_iter > 1 ? 1u : 0u;
         NA_CK(run(K_G2P_PBMPM));
     }
+    // the advanced state back into the caller's records
+    k_work_store<<<work_grid(n_particles), 256, 0, s>>>(c.work_out, c.ids_out, n_particles, (float4*)particles);
+    NA_CK(cudaGetLastError());
     if (status_out) {
         Counters ct;
         NA_CK(cudaMemcpyAsync(&ct, c.counters, sizeof(ct), cudaMemcpyDeviceToHost, s));

@@ -1,11 +1,16 @@
 // mpm_engine.cuh -- device-side data layout of the MPM step.
 //
 // HBM layout (all buffers allocated once by mpm_create):
-//   particles   N x 192 B  reference ParticleData records, never reordered
-//   order[2]    N x u32    particle ids in the previous substep's tile order
-//   bin_slot    N x u32    tile hash slot of the particle at order position t
+//   particles   N x 192 B  reference ParticleData records in the caller's order
+//                          (the boundary: loaded into, and stored back from, work)
+//   work[2]     REC_PLANES x N float4   the particle state the substeps advance,
+//                          plane by plane (word q of the 192-byte record of slot t
+//                          at work[q * N + t]), slots in the previous substep's tile
+//                          order; each substep reads one and writes the other
+//   ids[2]      N x u32    caller index of each work slot
+//   bin_slot    N x u32    tile hash slot of the particle in work slot t
 //   bin_rank    N x u32    its rank inside that tile
-//   sorted      = order[next]: particle ids grouped by tile
+//   sorted      N x u32    work slots grouped by tile (this substep's tile order)
 //   keys        cap x u64  open-addressing tile hash (hash3 of the tile coord,
 //                          linear probing); EMPTY = ~0
 //   slot_count  cap x u32  particles per slot
@@ -45,6 +50,8 @@ constexpr int KEY_BIAS = 32768;
 // substep, so Fe^-1 and the relaxation factor (pbmpm.wgsl:29-35) are formed
 // once, by the first iteration, instead of once per iteration.
 constexpr int IR_PLANES = 6;
+// Float4 words of a particle record (192 B), one plane each in the work buffers.
+constexpr int REC_PLANES = 12;
 
 // status bits (mirror of MPM_STATUS_* in include/mpm.h)
 constexpr uint32_t ST_HASH_FULL = 0x1u;
@@ -124,13 +131,16 @@ struct Counters {
     uint32_t step;       // substeps run on this buffer (advanced at each substep's start)
     uint32_t tile_ticket;  // tile kernels: tiles claimed past each CTA's first (0 between launches)
     uint32_t tile_done;    // tile kernels: CTAs finished; the last one resets both
-    uint32_t pad;
+    uint32_t n_carry;      // particles no tile kernel advances this substep (no hash slot):
+                           // copied unchanged into work slots n_binned, n_binned + 1, ...
 };
 
 struct Ctx {
-    float4* particles;        // N x 12 float4
-    const uint32_t* order_in; // previous tile order
-    uint32_t* sorted;         // this substep's tile order
+    const float4* work_in;    // particle state before the substep: REC_PLANES planes of n float4
+    float4* work_out;         // after the substep, slots in this substep's tile order
+    const uint32_t* ids_in;   // caller index of each slot of work_in
+    uint32_t* ids_out;        // caller index of each slot of work_out
+    uint32_t* sorted;         // slots of work_in grouped by tile (this substep's tile order)
     uint32_t* bin_slot;
     uint32_t* bin_rank;
     unsigned long long* keys;
@@ -154,7 +164,7 @@ struct Ctx {
     const int4* tiles_m;      // readback only: tiles holding the substep's mass sums (nullptr: tiles_b)
     uint32_t iter_first;      // this PBMPM iteration forms and stores the reciprocal masses
     uint32_t g2p_rm;          // the final PBMPM G2P reads the stored reciprocal masses
-    uint32_t* plast_list;     // deferred plasticity: particles the strain-bound check did not clear
+    uint32_t* plast_list;     // deferred plasticity: work_out slots the strain-bound check did not clear
     uint32_t plast_defer;     // 0: exact return map inside integrate; 1: deferred to the plasticity pass
     const SceneDev* scenes;
     const uint32_t* scene_first;  // n_scenes + 1 particle offsets

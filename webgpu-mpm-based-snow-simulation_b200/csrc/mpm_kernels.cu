@@ -99,7 +99,8 @@ __device__ __forceinline__ void grid_bc(const SceneDev& S, const int* gc, float*
 }
 
 // ------------------------------------------------------------------
-// particle record access (192 B = 12 float4)
+// particle state access: the 192-byte record (12 float4 words, the
+// reference's ParticleData layout) of work slot t, word q at w[q * n + t]
 // ------------------------------------------------------------------
 struct PState {
     float pos[3], hom, vel[3], mass;
@@ -118,35 +119,39 @@ __device__ __forceinline__ float4 ld4(const float4* p) {
     return *p;
 }
 
-// loads record words [0, nq) float4s
+// loads record words 0..7 (position, velocity, mass, Fe, Fp) and, with
+// want_dx_d, words 8..11 (displacement, D) of work slot t
 template <bool RO>
-__device__ __forceinline__ void load_particle(const float4* rec, PState& s, bool want_vel, bool want_dx_d) {
-    float4 q0 = ld4<RO>(rec + 0), q1 = ld4<RO>(rec + 1);
+__device__ __forceinline__ void load_particle(const float4* w, size_t n, uint32_t t, PState& s, bool want_dx_d) {
+    const float4* r = w + t;
+    float4 q0 = ld4<RO>(r), q1 = ld4<RO>(r + n);
     s.pos[0] = q0.x; s.pos[1] = q0.y; s.pos[2] = q0.z; s.hom = q0.w;
     s.vel[0] = q1.x; s.vel[1] = q1.y; s.vel[2] = q1.z; s.mass = q1.w;
-    (void)want_vel;
-    unpack_m(ld4<RO>(rec + 2), ld4<RO>(rec + 3), ld4<RO>(rec + 4), s.Fe);
-    unpack_m(ld4<RO>(rec + 5), ld4<RO>(rec + 6), ld4<RO>(rec + 7), s.Fp);
+    unpack_m(ld4<RO>(r + 2 * n), ld4<RO>(r + 3 * n), ld4<RO>(r + 4 * n), s.Fe);
+    unpack_m(ld4<RO>(r + 5 * n), ld4<RO>(r + 6 * n), ld4<RO>(r + 7 * n), s.Fp);
     if (want_dx_d) {
-        float4 q8 = ld4<RO>(rec + 8);
+        float4 q8 = ld4<RO>(r + 8 * n);
         s.dxp[0] = q8.x; s.dxp[1] = q8.y; s.dxp[2] = q8.z;
-        unpack_m(ld4<RO>(rec + 9), ld4<RO>(rec + 10), ld4<RO>(rec + 11), s.D);
+        unpack_m(ld4<RO>(r + 9 * n), ld4<RO>(r + 10 * n), ld4<RO>(r + 11 * n), s.D);
     }
 }
 
-__device__ __forceinline__ void store_particle(float4* rec, const PState& s) {
-    rec[0] = make_float4(s.pos[0], s.pos[1], s.pos[2], s.hom);
-    rec[1] = make_float4(s.vel[0], s.vel[1], s.vel[2], s.mass);
-    rec[2] = make_float4(s.Fe[0], s.Fe[1], s.Fe[2], 0.f);
-    rec[3] = make_float4(s.Fe[3], s.Fe[4], s.Fe[5], 0.f);
-    rec[4] = make_float4(s.Fe[6], s.Fe[7], s.Fe[8], 0.f);
-    rec[5] = make_float4(s.Fp[0], s.Fp[1], s.Fp[2], 0.f);
-    rec[6] = make_float4(s.Fp[3], s.Fp[4], s.Fp[5], 0.f);
-    rec[7] = make_float4(s.Fp[6], s.Fp[7], s.Fp[8], 0.f);
-    rec[8] = make_float4(s.dxp[0], s.dxp[1], s.dxp[2], 0.f);
-    rec[9] = make_float4(s.D[0], s.D[1], s.D[2], 0.f);
-    rec[10] = make_float4(s.D[3], s.D[4], s.D[5], 0.f);
-    rec[11] = make_float4(s.D[6], s.D[7], s.D[8], 0.f);
+// the record words a G2P + integrate writes (padding words 0, the position's
+// fourth word kept), streamed past L1
+__device__ __forceinline__ void store_particle(float4* w, size_t n, uint32_t t, const PState& s) {
+    float4* r = w + t;
+    __stcs(r, make_float4(s.pos[0], s.pos[1], s.pos[2], s.hom));
+    __stcs(r + n, make_float4(s.vel[0], s.vel[1], s.vel[2], s.mass));
+    __stcs(r + 2 * n, make_float4(s.Fe[0], s.Fe[1], s.Fe[2], 0.f));
+    __stcs(r + 3 * n, make_float4(s.Fe[3], s.Fe[4], s.Fe[5], 0.f));
+    __stcs(r + 4 * n, make_float4(s.Fe[6], s.Fe[7], s.Fe[8], 0.f));
+    __stcs(r + 5 * n, make_float4(s.Fp[0], s.Fp[1], s.Fp[2], 0.f));
+    __stcs(r + 6 * n, make_float4(s.Fp[3], s.Fp[4], s.Fp[5], 0.f));
+    __stcs(r + 7 * n, make_float4(s.Fp[6], s.Fp[7], s.Fp[8], 0.f));
+    __stcs(r + 8 * n, make_float4(s.dxp[0], s.dxp[1], s.dxp[2], 0.f));
+    __stcs(r + 9 * n, make_float4(s.D[0], s.D[1], s.D[2], 0.f));
+    __stcs(r + 10 * n, make_float4(s.D[3], s.D[4], s.D[5], 0.f));
+    __stcs(r + 11 * n, make_float4(s.D[6], s.D[7], s.D[8], 0.f));
 }
 
 // cell number, fractional position, quadratic B-spline weights
@@ -552,6 +557,7 @@ __global__ void k_clear_table(Ctx c) {
         c.counters->step += 1u;
         c.counters->tile_ticket = 0u;
         c.counters->tile_done = 0u;
+        c.counters->n_carry = 0u;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t s = c.st_slot[i];
@@ -568,9 +574,8 @@ __global__ void __launch_bounds__(256) k_bin_insert(Ctx c) {
     uint32_t scene = 0;
     int st[3] = {0, 0, 0};
     if (act) {
-        uint32_t p = c.order_in[t];
-        float4 q0 = __ldg(c.particles + (size_t)p * 12);
-        scene = find_scene(c, p);
+        float4 q0 = __ldg(c.work_in + t);
+        scene = c.n_scenes > 1u ? find_scene(c, __ldg(c.ids_in + t)) : 0u;
         const SceneDev* S = c.scenes + scene;
         float pos[3] = {q0.x, q0.y, q0.z};
 #pragma unroll
@@ -710,12 +715,30 @@ __global__ void __launch_bounds__(256) k_compact_c(Ctx c) {
     }
 }
 
+// Places work slot t at its position in this substep's tile order.  A
+// particle that no tile kernel will advance (no hash slot, or a tile past the
+// tile storage: both reported in the status) is copied unchanged to its
+// output slot, so the state stays complete.
 __global__ void __launch_bounds__(256) k_bin_scatter(Ctx c) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= c.n_particles) return;
     uint32_t slot = c.bin_slot[t];
-    if (slot == INVALID) return;
-    c.sorted[c.slot_off[slot] + c.bin_rank[t]] = c.order_in[t];
+    uint32_t dst;
+    bool carry;
+    if (slot == INVALID) {
+        dst = c.counters->n_binned + atomicAdd(&c.counters->n_carry, 1u);
+        carry = true;
+    } else {
+        dst = c.slot_off[slot] + c.bin_rank[t];
+        c.sorted[dst] = t;
+        carry = c.slot_st[slot] >= c.max_tiles;
+    }
+    if (carry) {
+        const size_t n = c.n_particles;
+#pragma unroll
+        for (int q = 0; q < REC_PLANES; q++) c.work_out[q * n + dst] = c.work_in[q * n + t];
+        c.ids_out[dst] = c.ids_in[t];
+    }
 }
 
 // ------------------------------------------------------------------
@@ -1551,7 +1574,7 @@ __global__ void __launch_bounds__(BS) k_p2g_explicit(Ctx c) {
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
             uint32_t pid = c.sorted[begin + i];
             PState p;
-            load_particle<true>(c.particles + (size_t)pid * 12, p, true, false);
+            load_particle<true>(c.work_in, c.n_particles, pid, p, false);
             Stencil sc;
             make_stencil(S, p.pos, sc);
             int l0[3];
@@ -1637,17 +1660,18 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
         __syncthreads();
         uint32_t begin = c.st_begin[st], cnt = c.st_count[st];
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
-            uint32_t pid = c.sorted[begin + i];
-            float4* rec = c.particles + (size_t)pid * 12;
+            const uint32_t slot = begin + i;
+            const uint32_t pid = c.sorted[slot];
             PState p;
-            load_particle<false>(rec, p, false, false);
+            load_particle<true>(c.work_in, c.n_particles, pid, p, false);
             Stencil sc;
             make_stencil(S, p.pos, sc);
             float nv[3], G[9];
             g2p_gather<E, PB>(T, vel, sc, nv, G);
             g2p_finish<PB>(S, nv, G, p.vel, p.dxp, p.D);
-            integrate(c, S, p, pid);
-            store_particle(rec, p);
+            integrate(c, S, p, slot);
+            store_particle(c.work_out, c.n_particles, slot, p);
+            c.ids_out[slot] = __ldg(c.ids_in + pid);
         }
         if (threadIdx.x == 0) s_next = claim_tile(c, n_st);
         __syncthreads();
@@ -1703,7 +1727,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
         for (uint32_t i = threadIdx.x; i < cnt; i += BS) {
             uint32_t pid = c.sorted[begin + i];
             PState p;
-            load_particle<true>(c.particles + (size_t)pid * 12, p, false, true);
+            load_particle<true>(c.work_in, c.n_particles, pid, p, true);
             float Fei[9];
             inv3(p.Fe, Fei);
             float relax = pbmpm_relax(S, p.Fp);

@@ -16,15 +16,17 @@
 //                         6 floats per vertex.
 // Arithmetic follows the WGSL expressions operation by operation (-fmad=false).
 //
+// The case table is the reference's (triTable.wgsl, prelude.wgsl
+// MC_TRI_COUNTS), written into mpm_mc_table.h by gen_mc_table.py: it fixes
+// which triangles each cube case emits and in which vertex order.  The cube's
+// vertex and edge numbering is the reference's (vertex bits x, z, y; edges
+// along x, then y, then z).
+//
 // Differences by design: the active blocks are compacted in ascending order
 // and triangles are placed by prefix sums (block, then cell, then table
-// order) instead of atomics, so the vertex buffer is deterministic; the
-// vertex densities of a block live in a per-block workspace instead of a
-// dense (res+1)^3 array; and the triangulation table is generated here
-// (mc_build_tables) by tracing the iso-contour around the cube with one
-// consistent rule for ambiguous faces (inside corners kept apart), which
-// makes every mesh closed.  The cube's vertex and edge numbering is the
-// reference's (vertex bits x, z, y; edges along x, then y, then z).
+// order) instead of atomics, so the vertex buffer is deterministic (the
+// reference's order depends on workgroup timing); the vertex densities of a
+// block live in a per-block workspace instead of a dense (res+1)^3 array.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,6 +37,7 @@
 
 #include "mpm_engine.cuh"
 #include "mpm_math.cuh"
+#include "mpm_mc_table.h"
 
 namespace mpm {
 
@@ -47,7 +50,6 @@ struct McTables {
 namespace {
 
 int cube_vertex(int x, int y, int z) { return x + 2 * z + 4 * y; }
-void cube_pos(int v, int* p) { p[0] = v & 1; p[1] = (v >> 2) & 1; p[2] = (v >> 1) & 1; }
 
 McTables build_tables() {
     McTables T;
@@ -65,68 +67,11 @@ McTables build_tables() {
             T.ev[e][1] = (uint8_t)cube_vertex(p1[0], p1[1], p1[2]);
         }
     }
-    auto edge_of = [&](int u, int v) {
-        for (int e = 0; e < 12; e++)
-            if ((T.ev[e][0] == u && T.ev[e][1] == v) || (T.ev[e][0] == v && T.ev[e][1] == u)) return e;
-        return -1;
-    };
-    // faces: corners counter-clockwise seen from outside
-    int face[6][4];
-    for (int a = 0, f = 0; a < 3; a++)
-        for (int s = 0; s < 2; s++, f++) {
-            int b = (a + 1) % 3, c = (a + 2) % 3;
-            int u = s ? b : c, w = s ? c : b;
-            int n = 0;
-            for (int v = 0; v < 8; v++) {
-                int p[3];
-                cube_pos(v, p);
-                if (p[a] == s) face[f][n++] = v;
-            }
-            std::sort(face[f], face[f] + 4, [&](int v0, int v1) {
-                int p[3], q[3];
-                cube_pos(v0, p);
-                cube_pos(v1, q);
-                return std::atan2(p[w] - 0.5, p[u] - 0.5) < std::atan2(q[w] - 0.5, q[u] - 0.5);
-            });
-        }
+    // the reference's case table (data contract: it fixes the triangles and
+    // their vertex order, so the vertex buffer equals the reference's)
     for (int cs = 0; cs < 256; cs++) {
-        int next[12];
-        for (int e = 0; e < 12; e++) next[e] = -1;
-        for (int f = 0; f < 6; f++) {
-            int typ[4], eid[4];
-            for (int i = 0; i < 4; i++) {
-                int a = face[f][i], b = face[f][(i + 1) % 4];
-                bool ia = (cs >> a) & 1, ib = (cs >> b) & 1;
-                eid[i] = edge_of(a, b);
-                typ[i] = (ia && !ib) ? 1 : ((!ia && ib) ? -1 : 0);
-            }
-            // each exit joins the entry that opened its run of inside corners
-            for (int i = 0; i < 4; i++) {
-                if (typ[i] != 1) continue;
-                int j = i;
-                do { j = (j + 3) % 4; } while (typ[j] != -1);
-                next[eid[i]] = eid[j];
-            }
-        }
-        bool seen[12] = {false};
-        int n = 0;
-        for (int e = 0; e < 12; e++) {
-            if (next[e] < 0 || seen[e]) continue;
-            int loop[12], k = 0;
-            for (int x = e; !seen[x]; x = next[x]) {
-                seen[x] = true;
-                loop[k++] = x;
-            }
-            // fan with the winding of the reference (right-hand normal towards the inside corner)
-            for (int t = 1; t + 1 < k; t++) {
-                T.tri[cs][3 * n + 0] = (int8_t)loop[0];
-                T.tri[cs][3 * n + 1] = (int8_t)loop[t];
-                T.tri[cs][3 * n + 2] = (int8_t)loop[t + 1];
-                n++;
-            }
-        }
-        T.count[cs] = (uint8_t)n;
-        for (int i = 3 * n; i < 16; i++) T.tri[cs][i] = -1;
+        std::memcpy(T.tri[cs], MPM_MC_TRI_TABLE[cs], 16);
+        T.count[cs] = MPM_MC_TRI_COUNTS[cs];
     }
     return T;
 }

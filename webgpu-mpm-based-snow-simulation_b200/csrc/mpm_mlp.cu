@@ -166,20 +166,23 @@ __device__ __forceinline__ void warp_count(unsigned long long* dst, bool pred) {
     if (b && (threadIdx.x & 31) == (uint32_t)(__ffs(__activemask()) - 1)) atomicAdd(dst, (unsigned long long)__popc(b));
 }
 
-__device__ __forceinline__ void load_fe_fp(const float4* rec, float* Fe, float* Fp) {
-    float4 q2 = rec[2], q3 = rec[3], q4 = rec[4], q5 = rec[5], q6 = rec[6], q7 = rec[7];
+// Fe and Fp of work slot t (record words 2..7; word q of slot t at w[q * n + t])
+__device__ __forceinline__ void load_fe_fp(const float4* w, size_t n, uint32_t t, float* Fe, float* Fp) {
+    const float4* rec = w + t;
+    float4 q2 = rec[2 * n], q3 = rec[3 * n], q4 = rec[4 * n], q5 = rec[5 * n], q6 = rec[6 * n], q7 = rec[7 * n];
     Fe[0] = q2.x; Fe[1] = q2.y; Fe[2] = q2.z; Fe[3] = q3.x; Fe[4] = q3.y; Fe[5] = q3.z;
     Fe[6] = q4.x; Fe[7] = q4.y; Fe[8] = q4.z;
     Fp[0] = q5.x; Fp[1] = q5.y; Fp[2] = q5.z; Fp[3] = q6.x; Fp[4] = q6.y; Fp[5] = q6.z;
     Fp[6] = q7.x; Fp[7] = q7.y; Fp[8] = q7.z;
 }
-__device__ __forceinline__ void store_fe_fp(float4* rec, const float* Fe, const float* Fp) {
-    rec[2] = make_float4(Fe[0], Fe[1], Fe[2], 0.f);
-    rec[3] = make_float4(Fe[3], Fe[4], Fe[5], 0.f);
-    rec[4] = make_float4(Fe[6], Fe[7], Fe[8], 0.f);
-    rec[5] = make_float4(Fp[0], Fp[1], Fp[2], 0.f);
-    rec[6] = make_float4(Fp[3], Fp[4], Fp[5], 0.f);
-    rec[7] = make_float4(Fp[6], Fp[7], Fp[8], 0.f);
+__device__ __forceinline__ void store_fe_fp(float4* w, size_t n, uint32_t t, const float* Fe, const float* Fp) {
+    float4* rec = w + t;
+    rec[2 * n] = make_float4(Fe[0], Fe[1], Fe[2], 0.f);
+    rec[3 * n] = make_float4(Fe[3], Fe[4], Fe[5], 0.f);
+    rec[4 * n] = make_float4(Fe[6], Fe[7], Fe[8], 0.f);
+    rec[5 * n] = make_float4(Fp[0], Fp[1], Fp[2], 0.f);
+    rec[6 * n] = make_float4(Fp[3], Fp[4], Fp[5], 0.f);
+    rec[7 * n] = make_float4(Fp[6], Fp[7], Fp[8], 0.f);
 }
 
 __device__ __forceinline__ uint32_t find_scene_p(const Ctx& c, uint32_t p) {
@@ -211,11 +214,12 @@ __global__ void __launch_bounds__(128) k_plasticity_exact(Ctx c, PlastCtx pc) {
     const uint32_t step = c.counters->step;
     {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-            uint32_t pid = c.plast_list[i];
-            float4* rec = c.particles + (size_t)pid * 12;
+            // the listed work slot; sampling and scene lookup use the caller's particle index
+            const uint32_t slot = c.plast_list[i];
+            const uint32_t pid = c.ids_out[slot];
             const SceneDev& S = c.scenes[find_scene_p(c, pid)];
             float Fe[9], Fp[9], x[12];
-            load_fe_fp(rec, Fe, Fp);
+            load_fe_fp(c.work_out, c.n_particles, slot, Fe, Fp);
             bool dom = mlp_features(Fe, Fp, S.dt, 1.0f - S.smin, x);
             warp_count(&pc.stats->candidates, true);
             warp_count(&pc.stats->fallback_domain, !dom);
@@ -231,7 +235,7 @@ __global__ void __launch_bounds__(128) k_plasticity_exact(Ctx c, PlastCtx pc) {
                     for (int k = 0; k < 10; k++) pc.pair_t[(size_t)slot * 10 + k] = t[k];
                 }
             }
-            store_fe_fp(rec, Fe2, Fp2);
+            store_fe_fp(c.work_out, c.n_particles, slot, Fe2, Fp2);
         }
     }
 }
@@ -255,8 +259,8 @@ __global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) 
     for (uint32_t tile = blockIdx.x; tile < n_tiles && alive; tile += gridDim.x) {
         const uint32_t idx = tile * ROWS + threadIdx.x;
         const bool valid = idx < count;
-        uint32_t pid = valid ? c.plast_list[idx] : 0u;
-        float4* rec = c.particles + (size_t)pid * 12;
+        const uint32_t slot = valid ? c.plast_list[idx] : 0u;
+        const uint32_t pid = valid ? c.ids_out[slot] : 0u;
         float Fe[9], Fp[9], x[12] = {0.f};
         bool dom = false;
         float smin = 0.f, smax = 0.f;
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) 
             const SceneDev& S = c.scenes[find_scene_p(c, pid)];
             smin = S.smin;
             smax = S.smax;
-            load_fe_fp(rec, Fe, Fp);
+            load_fe_fp(c.work_out, c.n_particles, slot, Fe, Fp);
             dom = mlp_features(Fe, Fp, S.dt, 1.0f - S.smin, x);
             if (!dom)
                 for (int k = 0; k < IN; k++) x[k] = 0.f;
@@ -304,9 +308,9 @@ __global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) 
                 atomicMax(&pc.stats->audit_max_err_bits, __float_as_uint(err));
                 atomicAdd(&pc.stats->audit_err_sum, (double)err);
             }
-            store_fe_fp(rec, Fe2, Fp2);
+            store_fe_fp(c.work_out, c.n_particles, slot, Fe2, Fp2);
         } else {
-            store_fe_fp(rec, Fn, Fpn);
+            store_fe_fp(c.work_out, c.n_particles, slot, Fn, Fpn);
         }
     }
     tc::fence_before_sync();
