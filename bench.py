@@ -594,8 +594,9 @@ def batched_leg(pkg, args, local, stream):
     specs = pkg.scenes.c3_batched()
     method = pkg.GpuSimulationMethodType.ExplicitMpm
     n_total = int(sum(s.particles.shape[0] for s in specs))
-    best, times = pkg.batching.autotune_tile_edge(specs, method, steps=3, device=local)
-    b = pkg.GpuMpmBatch(specs, device=local, tile_edge=best, stream=stream.cuda_stream)
+    sched, times = pkg.batching.autotune_schedule(specs, method, steps=3, device=local)
+    best = sched["tile_edge"]
+    b = pkg.GpuMpmBatch(specs, device=local, stream=stream.cuda_stream, **sched)
     steps = max(10, min(args.steps, 30))
     ms = pkg.batching.time_batch(b, method, steps, warmup=3)
     b.close()
@@ -619,10 +620,83 @@ def batched_leg(pkg, args, local, stream):
     for buf, _ in handles:
         buf.close()
     return {"workload": f"c3_batched: {len(specs)} scenes, {n_total:,} particles, explicit, dx 1/64 or 1/128",
-            "tile_edge_autotuned": best, "autotune_ms_per_substep": {str(k): round(v, 4) for k, v in times.items()},
+            "schedule_autotuned": sched, "autotune_ms_per_substep": {str(k): round(v, 4) for k, v in times.items()},
             "batched_ms_per_substep": round(ms, 4), "batched_value": n_total / (ms * 1e-3),
             "per_scene_loop_ms_per_substep": round(loop_ms, 4), "per_scene_loop_value": n_total / (loop_ms * 1e-3),
             "batched_vs_loop": loop_ms / ms, "unit": "particle-substeps/s"}
+
+
+def batched_sharded(args, rank, world, local):
+    """Config 3 sharded by scene over the ranks (`--batched`): each rank
+    advances its shard of the 256 scenes (shard_scenes: balanced by particle
+    count, the same on every rank, no communication) in one GpuMpmBatch;
+    CUDA events around K substeps, the max over ranks; the per-scene
+    aggregates are gathered on rank 0 afterwards (host objects, outside the
+    timed region).  The total work is fixed as N grows: strong scaling."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module(PKG)
+    specs = pkg.scenes.c3_batched()
+    counts = [int(s.particles.shape[0]) for s in specs]
+    mine = pkg.batching.shard_scenes(counts, world)[rank]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    method = pkg.GpuSimulationMethodType.ExplicitMpm
+    b = pkg.GpuMpmBatch([specs[i] for i in mine], device=local, tile_edge=args.tile_edge, stream=stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        b.step(method, 1)
+    b.mpm.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.step(method, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    status = b.mpm.sync()
+    rec = b.mpm.read_particles()
+    local_aggs = {i: pkg.batching.scene_aggregates(b.scene_particles(j, rec)) for j, i in enumerate(mine)}
+    b.close()
+    aggs = local_aggs
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        parts = [None] * world
+        dist.all_gather_object(parts, local_aggs)
+        aggs = {}
+        for part in parts:
+            aggs.update(part)
+    total = int(sum(counts))
+    return {
+        "metric": "particle-substeps/s, config 3 (256 independent scenes, sharded by scene)",
+        "value": total * args.steps / (ms * 1e-3), "unit": "particle-substeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32 (fixed-point i32 grid)",
+        "data": "synthetic (seeded procedural scenes; no dataset)",
+        "config": {"workload": f"c3_batched: {len(specs)} scenes, {total:,} particles, explicit, dx 1/64 or 1/128",
+                   "tile_edge": args.tile_edge, "parallelism": f"scenes sharded x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (2.2 GB of particle records)"},
+        "shard_particles_rank0": int(sum(counts[i] for i in mine)) if rank == 0 else None,
+        "scenes_gathered": len(aggs),
+        "aggregate_checksum": float(np.sum([v[0] + v[1] + v[2] for v in aggs.values()])),
+        "clocks": clk, "device_status": status,
+    }
 
 
 def _agg_any(rec):
@@ -783,6 +857,8 @@ def main():
                     help="measure configs 0-2 against the f32 and f64 oracles (one JSON line per config)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the learned-plasticity and batched-scene legs (they run at N = 1 only)")
+    ap.add_argument("--batched", action="store_true",
+                    help="config 3 instead: 256 independent scenes sharded by scene over the ranks")
     ap.add_argument("--counts", default="256,64,256",
                     help="slab lattice size x,y,z (default: the full 4,194,304-particle workload; smaller "
                          "lattices give the small cases used for profiling)")
@@ -817,6 +893,17 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.batched:
+        if args.tile_edge == 16:
+            args.tile_edge = 8   # the edge the autotuner picks for these scenes
+        out = batched_sharded(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     out = gpu_run(args, rank, world, local)
     if world == 1 and not args.no_extra:
         import torch

@@ -180,6 +180,14 @@ const char* mpm_kernel_name(uint32_t kernel_id);
 uint32_t mpm_kernel_count(void);
 /* Captures each substep into a CUDA graph (default on). */
 int mpm_use_graphs(MpmHandle* h, int enable);
+/* Schedule knobs (an extension; the reference dispatches fixed 4^3-block
+ * workgroups, sparseGridPrelude.wgsl:1-7), set by the autotuner.  The
+ * results do not depend on them.  order_mode: the order the tile kernels
+ * claim tiles in -- 0 automatic (compact order up to 256 occupied tiles,
+ * Morton buckets of 4 bits per axis up to 4,096, else 5), 1 compact order,
+ * 4 or 5 Morton buckets of that many bits per axis.  tile_block: threads per
+ * CTA of the explicit tile kernels, 0 or 256 (default) or 128. */
+int mpm_set_schedule(MpmHandle* h, uint32_t order_mode, uint32_t tile_block);
 /* Device self-test of the step's arithmetic helpers, on n pseudo-random
  * operand pairs: the folded fixed-point encoding i32(x * (r * 2^k)) against
  * i32((x * r) * 2^k), and the device reciprocal against the IEEE quotient

@@ -58,7 +58,7 @@ using namespace mpm;
 static const char* kKernelNames[K_COUNT] = {
     "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
     "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense",
-    "tile_nbr", "plasticity", "tile_order"};
+    "tile_nbr", "plasticity", "tile_order", "p2g_explicit_b128", "g2p_explicit_integrate_b128"};
 
 struct TimedLaunch {
     uint32_t kid;
@@ -157,6 +157,8 @@ struct MpmHandle {
 
     int blocks_per_sm[K_COUNT] = {0};
 
+    uint32_t order_mode = 0;      // schedule knobs (mpm_set_schedule)
+    uint32_t tile_block = 0;
     bool use_graphs = true;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [method][parity]
     uint64_t graph_sig[2][2] = {{0, 0}, {0, 0}};
@@ -790,6 +792,7 @@ static Ctx make_ctx(MpmHandle* h, int cur) {
     c.iter_rec = h->iter_rec;
     c.st_nbr = h->st_nbr;
     c.tile_order = h->tile_order;
+    c.order_mode = h->order_mode;
     c.tile_rm = h->tile_rm;
     c.plast_list = h->plast_list;
     c.plast_defer = h->plast_mode != PLAST_INLINE ? 1u : 0u;
@@ -884,12 +887,13 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
     // before it (which wrote the tiles it reads)
     c.order_rev = 0u;
     if (method == MPM_METHOD_EXPLICIT) {
+        const bool b128 = h->tile_block == 128u;
         c.tiles_a = h->tiles[0];
-        L(K_P2G_EXPLICIT);
+        L(b128 ? K_P2G_EXPLICIT_128 : K_P2G_EXPLICIT);
         if (stop_p2g) { h->last_tiles = 0; return cudaSuccess; }
         c.tiles_b = h->tiles[0];
         c.order_rev = 1u;
-        L(K_G2P_EXPLICIT);
+        L(b128 ? K_G2P_EXPLICIT_128 : K_G2P_EXPLICIT);
         if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
         h->last_tiles = 0;
     } else {
@@ -992,6 +996,7 @@ static uint64_t graph_signature(MpmHandle* h) {
     s = s * 1315423911ull + (uint64_t)h->audit_threshold + (uint64_t)__builtin_bit_cast(uint32_t, h->unc_threshold) +
         ((uint64_t)__builtin_bit_cast(uint32_t, h->det_threshold) << 32);
     s = s * 1315423911ull + (uint64_t)(uintptr_t)h->plast_list;
+    s = s * 1315423911ull + (uint64_t)h->order_mode * 1024u + h->tile_block;
     return s | 1ull;
 }
 
@@ -1282,6 +1287,18 @@ extern "C" int mpm_scatter_particles(MpmHandle* h, const float* vertices, uint32
     if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, "scatter: %s", cudaGetErrorString(e));
     h->work_valid = false;
     h->records_stale = false;
+    return MPM_OK;
+}
+
+extern "C" int mpm_set_schedule(MpmHandle* h, uint32_t order_mode, uint32_t tile_block) {
+    if (!h) return MPM_ERR_ARG;
+    if (order_mode != 0u && order_mode != 1u && order_mode != 4u && order_mode != 5u)
+        return fail(h, MPM_ERR_ARG, "order_mode must be 0, 1, 4 or 5");
+    if (tile_block != 0u && tile_block != 128u && tile_block != 256u)
+        return fail(h, MPM_ERR_ARG, "tile_block must be 0, 128 or 256");
+    h->order_mode = order_mode;
+    h->tile_block = tile_block;
+    destroy_graphs(h);
     return MPM_OK;
 }
 

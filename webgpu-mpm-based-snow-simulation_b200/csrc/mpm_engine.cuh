@@ -160,6 +160,8 @@ struct Ctx {
     uint32_t* tile_order;     // optional: the order the tile kernels claim tiles in (Morton order of
                               // the tile coordinates, per scene); nullptr: compact index order
     uint32_t order_rev;       // this launch claims tile_order from its end (alternates per launch)
+    uint32_t order_mode;      // tile claim order: 0 automatic, 1 compact index order, 4 / 5 Morton
+                              // buckets of 4 / 5 bits per axis (schedule knob of the autotuner)
     float* tile_rm;           // per tile (E+2)^3 reciprocal cell masses of the substep (PBMPM iterations)
     const int4* tiles_m;      // readback only: tiles holding the substep's mass sums (nullptr: tiles_b)
     uint32_t iter_first;      // this PBMPM iteration forms and stores the reciprocal masses
@@ -202,6 +204,8 @@ enum KernelId : uint32_t {
     K_TILE_NBR,
     K_PLASTICITY,
     K_TILE_ORDER,
+    K_P2G_EXPLICIT_128,       // the explicit tile kernels with 128-thread CTAs (schedule knob)
+    K_G2P_EXPLICIT_128,
     K_COUNT
 };
 

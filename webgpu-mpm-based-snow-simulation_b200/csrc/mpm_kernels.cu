@@ -1508,13 +1508,15 @@ __global__ void __launch_bounds__(1024) k_tile_order(Ctx c) {
     uint32_t* hist = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ uint32_t warp_sum[32];
     const uint32_t n = n_tiles_now(c);
-    if (n <= TILE_ORDER_MIN) {
-        // few tiles: nearly all run at once, so their order gains nothing
+    uint32_t mode = c.order_mode;
+    // automatic: few tiles nearly all run at once, so their order gains
+    // nothing; up to 4,096 tiles 4 bits per axis (4,096 buckets), else 5 (32,768)
+    if (mode != 1u && mode != 4u && mode != 5u) mode = n <= TILE_ORDER_MIN ? 1u : (n <= 4096u ? 4u : 5u);
+    if (mode == 1u) {
         for (uint32_t i = threadIdx.x; i < n; i += 1024) c.tile_order[i] = i;
         return;
     }
-    // up to 4,096 tiles: 4 bits per axis (4,096 buckets), else 5 (32,768)
-    if (n <= 4096u) tile_order_sort<4>(c, n, hist, warp_sum);
+    if (mode == 4u) tile_order_sort<4>(c, n, hist, warp_sum);
     else tile_order_sort<5>(c, n, hist, warp_sum);
 }
 
@@ -1915,7 +1917,9 @@ size_t smem_bytes(uint32_t kid) {
         case K_P2G_EXPLICIT:
         case K_PBMPM_FIRST:
         case K_G2P_EXPLICIT:
-        case K_G2P_PBMPM: return 16 * NC;
+        case K_G2P_PBMPM:
+        case K_P2G_EXPLICIT_128:
+        case K_G2P_EXPLICIT_128: return 16 * NC;
         case K_PBMPM_ITER: return 32 * NC;
         default: return 0;
     }
@@ -1926,6 +1930,7 @@ constexpr int iter_block() { return E == 16 ? 512 : 256; }
 
 template <int E>
 int block_size(uint32_t kid) {
+    if (kid == K_P2G_EXPLICIT_128 || kid == K_G2P_EXPLICIT_128) return 128;
     return kid == K_PBMPM_ITER ? iter_block<E>() : BS_DEFAULT;
 }
 
@@ -1947,13 +1952,16 @@ int kernel_ptrs(uint32_t kid, void** out) {
             return 2;
         case K_GRID_DENSE: out[0] = (void*)k_grid_dense<E>; return 1;
         case K_TILE_NBR: out[0] = (void*)k_tile_nbr<E>; return 1;
+        case K_P2G_EXPLICIT_128: out[0] = (void*)k_p2g_explicit<E, 128>; return 1;
+        case K_G2P_EXPLICIT_128: out[0] = (void*)k_g2p_integrate<E, false, 128, 0>; return 1;
         default: return 0;
     }
 }
 
 template <int E>
 cudaError_t configure_tile_kernels(int* blocks_per_sm) {
-    for (uint32_t kid : {K_P2G_EXPLICIT, K_G2P_EXPLICIT, K_PBMPM_FIRST, K_PBMPM_ITER, K_G2P_PBMPM, K_GRID_DENSE}) {
+    for (uint32_t kid : {K_P2G_EXPLICIT, K_G2P_EXPLICIT, K_PBMPM_FIRST, K_PBMPM_ITER, K_G2P_PBMPM, K_GRID_DENSE,
+                         K_P2G_EXPLICIT_128, K_G2P_EXPLICIT_128}) {
         void* fs[2] = {nullptr, nullptr};
         int nf = kernel_ptrs<E>(kid, fs);
         size_t sm = smem_bytes<E>(kid);
@@ -1998,6 +2006,8 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
             break;
         case K_GRID_DENSE: k_grid_dense<E><<<grid_tiles, 256, 0, s>>>(c, scene, apply, out); break;
         case K_TILE_ORDER: if (c.tile_order) k_tile_order<<<1, 1024, TILE_ORDER_SMEM, s>>>(c); break;
+        case K_P2G_EXPLICIT_128: k_p2g_explicit<E, 128><<<grid_tiles, 128, smem_bytes<E>(kid), s>>>(c); break;
+        case K_G2P_EXPLICIT_128: k_g2p_integrate<E, false, 128, 0><<<grid_tiles, 128, smem_bytes<E>(kid), s>>>(c); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -454,14 +454,16 @@ class GpuMpmBatch:
     kernel once over all tiles, captured in one CUDA graph.  The reference
     runs one scene per device; this is the batched form of its step."""
 
-    def __init__(self, specs, *, device: int = 0, tile_edge: int = 16, stream: int | None = None):
+    def __init__(self, specs, *, device: int = 0, tile_edge: int = 16, stream: int | None = None,
+                 hash_capacity: int = 0, order_mode: int = 0, tile_block: int = 0):
         lib = load()
         self.specs = list(specs)
         counts = [int(s.particles.shape[0]) for s in self.specs]
         n = int(sum(counts))
         self.mpm = GpuMpmBufferManager(n_particles=n, device=device, max_scenes=len(self.specs),
-                                       tile_edge=tile_edge, stream=stream)
+                                       tile_edge=tile_edge, stream=stream, hash_capacity=hash_capacity)
         h = self.mpm.handle
+        check(lib.mpm_set_schedule(h, order_mode, tile_block), h)
         check(lib.mpm_set_scene_count(h, len(self.specs)), h)
         self.ranges = []
         first = 0
