@@ -89,6 +89,10 @@ typedef struct MpmParams {
     float collider_vel_scale;    /* colliderPrelude.wgsl:294: 0.2 */
     float pbmpm_blend;           /* pbmpm.wgsl:26: 0.95 */
     float pbmpm_volume_exponent; /* pbmpm.wgsl:23: -0.3333333 */
+    uint32_t return_map;         /* 0: applyPlasticity (plasticityOps.wgsl:7-48), the clamp of the
+                                  * diagonal of R^T Fe; 1: a true-SVD clamp of the singular values,
+                                  * an option of this library (applied by the deferred plasticity
+                                  * pass; not available to mpm_step_noalloc) */
 } MpmParams;
 
 /* ---- lifetime ------------------------------------------------------ */

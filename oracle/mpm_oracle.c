@@ -346,6 +346,7 @@ typedef struct Scene {
     int32_t bc;
     uint32_t gaxis;
     real cmargin, csurf, cthr, cfric, cvs, blend, vexp;
+    uint32_t rmap;   /* return map: 0 applyPlasticity, 1 SVD clamp (library option) */
     /* RN(1/d) of the substep-constant divisors (f32 instantiation), and
      * g*dt rounded once (gridUpdate.cs.wgsl:44) */
     real rdt, rcd[3], rscale, rfdiv, gdt[3];
@@ -402,6 +403,7 @@ static void load_scene(Scene* s, const uint8_t* u, const OrExt* e) {
     s->cvs = e->collider_vel_scale;
     s->blend = e->pbmpm_blend;
     s->vexp = e->pbmpm_volume_exponent;
+    s->rmap = e->return_map;
     s->rdt = (real)1 / s->dt;
     for (int i = 0; i < 3; i++) s->rcd[i] = (real)1 / s->cd[i];
     s->rscale = (real)1 / s->scale;
@@ -910,7 +912,13 @@ static void g2p(const OrCtx* c, const Scene* s, PS* p, int pbmpm) {
 /* ------------------------------------------------------------------ */
 /* plasticity (plasticityOps.wgsl:7-48)                                */
 /* ------------------------------------------------------------------ */
+static void plasticity_svd(const Scene* s, real* Fe, real* Fp);
+
 static void plasticity(const Scene* s, real* Fe, real* Fp) {
+    if (s->rmap == 1u) {
+        plasticity_svd(s, Fe, Fp);
+        return;
+    }
     real R[9], Rt[9], S[9];
     polar3(Fe, R);
     tr3(R, Rt);
@@ -923,6 +931,58 @@ static void plasticity(const Scene* s, real* Fe, real* Fp) {
     real Dg[9] = {sc[0], 0, 0, 0, sc[1], 0, 0, 0, sc[2]};
     real Fn[9], Fni[9], F[9], Fpn[9];
     mul3(R, Dg, Fn);
+    inv3(Fn, Fni);
+    mul3(Fe, Fp, F);
+    mul3(Fni, F, Fpn);
+    memcpy(Fe, Fn, sizeof(Fn));
+    memcpy(Fp, Fpn, sizeof(Fpn));
+}
+
+/* ------------------------------------------------------------------ */
+/* SVD return map (return_map 1): an option of this library, not the      */
+/* reference's map.  One-sided Jacobi SVD (M. R. Hestenes, "Inversion of  */
+/* matrices by biorthogonalization and related results", J. SIAM 6, 1958): */
+/* the column pairs (0,1), (0,2), (1,2) of A = Fe are rotated in 4 sweeps */
+/* until A V = U diag(sigma), sigma_k = |a_k|.  Every sigma in            */
+/* [smin, smax]: unchanged; else Fe' = sum_k (clamp(sigma_k) / sigma_k)    */
+/* a_k v_k^T and Fp' = Fe'^-1 (Fe Fp).  Same operations as plasticity_svd */
+/* in mpm_plast.cuh.                                                     */
+/* ------------------------------------------------------------------ */
+#define SVD_SWEEPS 4
+static inline void jrot(real* x, real* y, real c, real sn) {
+    for (int r = 0; r < 3; r++) {
+        real xr = x[r], yr = y[r];
+        x[r] = c * xr - sn * yr;
+        y[r] = sn * xr + c * yr;
+    }
+}
+static void plasticity_svd(const Scene* s, real* Fe, real* Fp) {
+    real a[9], v[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    memcpy(a, Fe, sizeof(a));
+    static const int P[3] = {0, 0, 1}, Q[3] = {1, 2, 2};
+    for (int sw = 0; sw < SVD_SWEEPS; sw++)
+        for (int k = 0; k < 3; k++) {
+            real* ap = a + 3 * P[k];
+            real* aq = a + 3 * Q[k];
+            real al = dot3(ap, ap), be = dot3(aq, aq), ga = dot3(ap, aq);
+            if (ga == (real)0) continue;
+            real ze = (be - al) / ((real)2 * ga);
+            real t = (signbit(ze) ? (real)-1 : (real)1) / (r_abs(ze) + r_sqrt(FMA(ze, ze, (real)1)));
+            real c = (real)1 / r_sqrt(FMA(t, t, (real)1));
+            real sn = c * t;
+            jrot(ap, aq, c, sn);
+            jrot(v + 3 * P[k], v + 3 * Q[k], c, sn);
+        }
+    real sg[3];
+    for (int k = 0; k < 3; k++) sg[k] = r_sqrt(dot3(a + 3 * k, a + 3 * k));
+    if (s->smin <= sg[0] && s->smin <= sg[1] && s->smin <= sg[2] &&
+        sg[0] <= s->smax && sg[1] <= s->smax && sg[2] <= s->smax) return;
+    real w[3];
+    for (int k = 0; k < 3; k++) w[k] = sg[k] > (real)0 ? r_min(r_max(sg[k], s->smin), s->smax) / sg[k] : (real)1;
+    real Fn[9], Fni[9], F[9], Fpn[9];
+    for (int j = 0; j < 3; j++)
+        for (int r = 0; r < 3; r++)
+            Fn[3 * j + r] = FMA((w[2] * a[6 + r]), v[6 + j], FMA((w[1] * a[3 + r]), v[3 + j], (w[0] * a[r]) * v[j]));
     inv3(Fn, Fni);
     mul3(Fe, Fp, F);
     mul3(Fni, F, Fpn);
@@ -1306,3 +1366,12 @@ void orf_plasticity(const OrExt* ext, float* Fe, float* Fp) {
     plasticity(&s, Fe, Fp);
 }
 #endif
+
+/* the selected return map on n states (f32: orf_, f64: ord_) */
+void PFX(plasticity_n)(const OrExt* ext, real* Fe, real* Fp, uint32_t n) {
+    uint8_t uni[OR_UNIFORMS_BYTES];
+    memset(uni, 0, sizeof(uni));
+    Scene s;
+    load_scene(&s, uni, ext);
+    for (uint32_t i = 0; i < n; i++) plasticity(&s, Fe + 9 * (size_t)i, Fp + 9 * (size_t)i);
+}

@@ -57,6 +57,7 @@ typedef struct OrExt {
     float collider_vel_scale;    /* colliderPrelude.wgsl:294: 0.2 */
     float pbmpm_blend;           /* pbmpm.wgsl:26: 0.95 */
     float pbmpm_volume_exponent; /* pbmpm.wgsl:23: -0.3333333 */
+    uint32_t return_map;         /* 0: applyPlasticity (plasticityOps.wgsl:7-48); 1: SVD clamp (library option) */
 } OrExt;
 
 /* 192-byte particle record, byte-for-byte the reference ParticleData

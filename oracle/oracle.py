@@ -38,7 +38,7 @@ class OrExt(C.Structure):
         ("boundary_mode", C.c_uint32), ("restitution", C.c_float), ("bc_cells", C.c_uint32),
         ("ground_axis", C.c_uint32), ("collider_margin", C.c_float), ("collider_surface_margin", C.c_float),
         ("collider_threshold", C.c_float), ("collider_friction", C.c_float), ("collider_vel_scale", C.c_float),
-        ("pbmpm_blend", C.c_float), ("pbmpm_volume_exponent", C.c_float),
+        ("pbmpm_blend", C.c_float), ("pbmpm_volume_exponent", C.c_float), ("return_map", C.c_uint32),
     ]
 
 
@@ -70,6 +70,7 @@ def lib():
             "or_powf": (C.c_float, [C.c_float, C.c_float]), "or_f2i": (C.c_int32, [C.c_float]),
             "orf_inverse": (None, [V, V]), "orf_polar": (None, [V, V]), "orf_det": (C.c_float, [V]),
             "orf_plasticity": (None, [V, V, V]),
+            "orf_plasticity_n": (None, [V, V, V, U32]), "ord_plasticity_n": (None, [V, V, V, U32]),
             "or_bvh_build": (U32, [V, U32, V, U32, V, V]),
             "or_mlp_forward": (None, [V, V, U32, I32, V]),
             "or_mlp_gradient": (C.c_double, [V, V, V, U32, C.c_float, I32, V]),
@@ -223,18 +224,32 @@ def mlp_gradient(params, x, t, unc_weight=0.1, bf16=True):
     return loss, g
 
 
-def mlp_pair(Fe, Fp, dt, theta_c, theta_s):
-    """(in_domain, x[12], t[10], Fe', Fp') of one trial state through the exact map."""
+def mlp_pair(Fe, Fp, dt, theta_c, theta_s, return_map=0):
+    """(in_domain, x[12], t[10], Fe', Fp') of one trial state through the exact
+    map (return_map 0: applyPlasticity; 1: the SVD clamp)."""
     fe = np.ascontiguousarray(Fe, np.float32).reshape(9)
     fp = np.ascontiguousarray(Fp, np.float32).reshape(9)
     x = np.zeros(12, np.float32)
     ok = lib().or_mlp_features(fe.ctypes.data, fp.ctypes.data, dt, theta_c, x.ctypes.data)
-    e = make_ext({"theta_c": theta_c, "theta_s": theta_s})
+    e = make_ext({"theta_c": theta_c, "theta_s": theta_s, "return_map": return_map})
     fe2, fp2 = fe.copy(), fp.copy()
     lib().orf_plasticity(C.byref(e), fe2.ctypes.data, fp2.ctypes.data)
     t = np.zeros(10, np.float32)
     lib().or_mlp_targets(fe.ctypes.data, fp.ctypes.data, fe2.ctypes.data, fp2.ctypes.data, t.ctypes.data)
     return bool(ok), x, t, fe2, fp2
+
+
+def return_map(Fe, Fp, params: dict, fp64: bool = False):
+    """The selected return map (params["return_map"]: 0 applyPlasticity, 1 the
+    SVD clamp) on states Fe, Fp [n, 3, 3] stored as 9 column-major entries:
+    (Fe', Fp')."""
+    dt = np.float64 if fp64 else np.float32
+    fe = np.ascontiguousarray(np.asarray(Fe, dt).reshape(-1, 9)).copy()
+    fp = np.ascontiguousarray(np.asarray(Fp, dt).reshape(-1, 9)).copy()
+    e = make_ext(params)
+    (lib().ord_plasticity_n if fp64 else lib().orf_plasticity_n)(C.byref(e), fe.ctypes.data, fp.ctypes.data,
+                                                                fe.shape[0])
+    return fe, fp
 
 
 def cert_elastic(Fe, theta_c, theta_s):

@@ -77,6 +77,25 @@ def test_deferred_exact_equals_inline(gpu, kind):
     b.close()
 
 
+@pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
+def test_svd_return_map_bit_exact(gpu, oracle_mod, kind):
+    """The SVD return map (return_map 1, an option of this library, applied by
+    the deferred plasticity pass) equals the oracle's restatement bit for
+    bit over several substeps with yielding; it is a different map from the
+    reference's (the states differ)."""
+    spec = _scene(gpu, kind)
+    spec.params["return_map"] = 1
+    g = GpuScene(gpu, spec)
+    assert g.step(4) == 0
+    got = g.particles()
+    g.close()
+    _, want = run_oracle(oracle_mod, spec, n_steps=4)
+    compare_states(got, want)
+    spec.params["return_map"] = 0
+    _, ref = run_oracle(oracle_mod, spec, n_steps=4)
+    assert not np.array_equal(got["Fe"], ref["Fe"])
+
+
 def _collect(gpu, specs, steps, cap):
     """Rollouts in COLLECT mode; returns the pairs (x, t) on the device."""
     torch = _torch()
@@ -94,8 +113,12 @@ def _collect(gpu, specs, steps, cap):
     return torch.cat(xs), torch.cat(ts)
 
 
-def test_collected_pairs_match_exact_map(gpu, oracle_mod):
+@pytest.mark.parametrize("return_map", [0, 1])
+def test_collected_pairs_match_exact_map(gpu, oracle_mod, return_map):
+    """COLLECT pairs: targets of the scene's return map (the reference's, or
+    the SVD clamp, on which a network that replaces the SVD map trains)."""
     spec = _scene(gpu, "explicit", seed=11)
+    spec.params["return_map"] = return_map
     # the collecting run itself follows the exact map: same states as inline
     a = GpuScene(gpu, spec)
     b = GpuScene(gpu, spec)
@@ -118,7 +141,7 @@ def test_collected_pairs_match_exact_map(gpu, oracle_mod):
         Fe = (xh[i, :9] / np.float32(20.0) + np.eye(3, dtype=np.float32).reshape(9)).astype(np.float32)
         jp = np.exp(xh[i, 9] / 2.0)
         Fp = (np.eye(3) * jp ** (1.0 / 3.0)).astype(np.float32).reshape(9)
-        ok, xo, to, _, _ = oracle_mod.mlp_pair(Fe, Fp, dt, 0.025, 7.5e-3)
+        ok, xo, to, _, _ = oracle_mod.mlp_pair(Fe, Fp, dt, 0.025, 7.5e-3, return_map)
         assert ok
         if not np.allclose(th[i, :9], to[:9], atol=2e-3):
             bad += 1

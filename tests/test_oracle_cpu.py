@@ -215,3 +215,40 @@ def test_bvh_leaves_cover_all_triangles(pkg):
     cnt = nodes[leaf, 7] & 0x7FFFFFFF
     assert cnt.max() <= 4 and cnt.sum() == f.size // 3
     assert sorted(order.tolist()) == list(range(f.size // 3))
+
+
+def test_svd_return_map_matches_numpy_svd(oracle_mod):
+    """The SVD return map (return_map 1, an option of this library): the f64
+    oracle equals a numpy SVD clamp of the singular values (Fe' = U clamp(S)
+    V^T, Fp' = Fe'^-1 Fe Fp) to 1e-8 (four Jacobi sweeps converge well below
+    f32 rounding); the f32 oracle is within 2e-6 of it;
+    states whose singular values are all inside the band come back unchanged
+    bit for bit."""
+    rng = np.random.default_rng(11)
+    n = 2000
+    Fe = np.eye(3)[None] + rng.normal(0.0, 0.03, (n, 3, 3))
+    Fp = np.eye(3)[None] + rng.normal(0.0, 0.01, (n, 3, 3))
+    prm = {"theta_c": 2.5e-2, "theta_s": 7.5e-3, "return_map": 1}
+    smin, smax = 1 - 2.5e-2, 1 + 7.5e-3
+    # 9 stored entries per matrix are column-major: entry 3c + r = M[r][c]
+    col = lambda M: np.ascontiguousarray(np.transpose(M, (0, 2, 1))).reshape(-1, 9)
+    uncol = lambda m: np.transpose(m.reshape(-1, 3, 3), (0, 2, 1))
+    fe64, fp64 = oracle_mod.return_map(col(Fe), col(Fp), prm, fp64=True)
+    U, S, Vt = np.linalg.svd(Fe)
+    Sc = np.clip(S, smin, smax)
+    want_fe = U @ (Sc[:, :, None] * Vt)
+    want_fp = np.linalg.inv(want_fe) @ Fe @ Fp
+    inside = np.all((S >= smin) & (S <= smax), axis=1)
+    got_fe, got_fp = uncol(fe64), uncol(fp64)
+    assert np.max(np.abs(got_fe - want_fe)) < 1e-8
+    assert np.max(np.abs(got_fp[~inside] - want_fp[~inside])) < 1e-8
+    fe32, fp32 = oracle_mod.return_map(col(Fe).astype(np.float32), col(Fp).astype(np.float32), prm)
+    assert np.max(np.abs(uncol(fe32).astype(np.float64) - want_fe)) < 2e-6
+    # a state well inside the band: unchanged, bit for bit
+    F0 = (np.eye(3) * 1.001).astype(np.float32).reshape(1, 9)
+    P0 = np.eye(3, dtype=np.float32).reshape(1, 9)
+    f, p = oracle_mod.return_map(F0, P0, prm)
+    assert np.array_equal(f.view(np.uint32), F0.view(np.uint32)) and np.array_equal(p.view(np.uint32), P0.view(np.uint32))
+    # the reference map (return_map 0) differs from the SVD clamp on sheared states
+    fr, _ = oracle_mod.return_map(col(Fe), col(Fp), dict(prm, return_map=0), fp64=True)
+    assert np.max(np.abs(uncol(fr) - want_fe)) > 1e-4

@@ -252,7 +252,7 @@ def test_device_upload_and_pointer(gpu, oracle_mod):
     assert g.buf.sync() == 0
 
     class _Raw:  # a view of the library's record buffer for torch
-        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, True), "version": 3}
+        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
 
     recs = torch.as_tensor(_Raw(), device="cuda").clone()
     compare_states(recs.cpu().numpy().view(spec.particles.dtype), want)

@@ -70,6 +70,7 @@ class MpmParams(C.Structure):
         ("collider_vel_scale", C.c_float),
         ("pbmpm_blend", C.c_float),
         ("pbmpm_volume_exponent", C.c_float),
+        ("return_map", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:

@@ -135,6 +135,7 @@ struct MpmHandle {
     uint32_t* tile_order = nullptr;  // max_tiles: the tile kernels' claim order
     // deferred / learned plasticity
     int plast_mode = PLAST_INLINE;
+    bool svd_any = false;          // some scene selects the SVD return map: plasticity runs deferred
     MpmMlp* mlp = nullptr;
     float unc_threshold = 0.05f, det_threshold = 1e-3f;
     uint32_t audit_threshold = 0;
@@ -296,6 +297,7 @@ static void build_scene_dev(SceneHost& s) {
     d.cvs = e.collider_vel_scale;
     d.blend = e.pbmpm_blend;
     d.vexp = e.pbmpm_volume_exponent;
+    d.rmap = e.return_map == 1u ? 1u : 0u;
     d.p_first = p_first;
     d.p_count = p_count;
     d.col_data = col;
@@ -753,6 +755,13 @@ static int upload_scenes(MpmHandle* h) {
         return fail(h, MPM_ERR_ARG, "scene ranges cover %u particles, buffer holds %u", expect, h->n_particles);
     first[h->n_scenes] = expect;
     h->scene_first = first;
+    bool svd = false;
+    for (uint32_t s = 0; s < h->n_scenes; s++) svd = svd || h->scenes[s].dev.rmap == 1u;
+    if (svd != h->svd_any) {
+        h->svd_any = svd;
+        destroy_graphs(h);
+    }
+    if (svd && !h->plast_list) CK(h, cudaMalloc(&h->plast_list, (size_t)h->cfg.max_particles * 4));
     std::vector<SceneDev> tmp(h->n_scenes);
     for (uint32_t s = 0; s < h->n_scenes; s++) tmp[s] = h->scenes[s].dev;
     CK(h, cudaMemcpyAsync(h->d_scenes, tmp.data(), tmp.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
@@ -795,7 +804,7 @@ static Ctx make_ctx(MpmHandle* h, int cur) {
     c.order_mode = h->order_mode;
     c.tile_rm = h->tile_rm;
     c.plast_list = h->plast_list;
-    c.plast_defer = h->plast_mode != PLAST_INLINE ? 1u : 0u;
+    c.plast_defer = (h->plast_mode != PLAST_INLINE || h->svd_any) ? 1u : 0u;
     c.scenes = h->d_scenes;
     c.scene_first = h->d_scene_first;
     c.counters = h->counters;
@@ -853,7 +862,9 @@ static cudaError_t launch(MpmHandle* h, uint32_t kid, const Ctx& c, bool capturi
         pc.pair_t = h->pair_t;
         pc.pair_count = h->d_pair_count;
         pc.pair_cap = h->pair_cap;
-        e = launch_plasticity(h->plast_mode, c, pc, h->n_sms * (h->plast_mode == PLAST_LEARNED ? 4 : 8), h->stream);
+        // INLINE with an SVD scene: the exact pass applies each scene's map
+        const int pm = h->plast_mode == PLAST_INLINE ? PLAST_EXACT : h->plast_mode;
+        e = launch_plasticity(pm, c, pc, h->n_sms * (pm == PLAST_LEARNED ? 4 : 8), h->stream);
     } else {
         e = launch_e(h->tile_edge, kid, c, h->stream, grid, 0, 0, nullptr);
     }
@@ -894,7 +905,7 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
         c.tiles_b = h->tiles[0];
         c.order_rev = 1u;
         L(b128 ? K_G2P_EXPLICIT_128 : K_G2P_EXPLICIT);
-        if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
+        if (h->plast_mode != PLAST_INLINE || h->svd_any) L(K_PLASTICITY);
         h->last_tiles = 0;
     } else {
         // tiles[0] keeps the first transfer (with the mass sums); the
@@ -917,7 +928,7 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
         c.g2p_rm = n_iter > 1 ? 1u : 0u;
         c.order_rev = n_iter & 1u;
         L(K_G2P_PBMPM);
-        if (h->plast_mode != PLAST_INLINE) L(K_PLASTICITY);
+        if (h->plast_mode != PLAST_INLINE || h->svd_any) L(K_PLASTICITY);
         h->last_tiles = cur;
     }
 #undef L
@@ -996,7 +1007,7 @@ static uint64_t graph_signature(MpmHandle* h) {
     s = s * 1315423911ull + (uint64_t)h->audit_threshold + (uint64_t)__builtin_bit_cast(uint32_t, h->unc_threshold) +
         ((uint64_t)__builtin_bit_cast(uint32_t, h->det_threshold) << 32);
     s = s * 1315423911ull + (uint64_t)(uintptr_t)h->plast_list;
-    s = s * 1315423911ull + (uint64_t)h->order_mode * 1024u + h->tile_block;
+    s = s * 1315423911ull + (uint64_t)h->order_mode * 1024u + h->tile_block + (h->svd_any ? 7u : 0u);
     return s | 1ull;
 }
 
@@ -1682,6 +1693,9 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     if (!uniforms || uniform_bytes < 544)
         return na_fail(err, err_len, MPM_ERR_ARG, "uniform block needs >= 544 bytes, got %zu", uniform_bytes);
     if (!params || params->n_iter == 0) return na_fail(err, err_len, MPM_ERR_ARG, "params missing or n_iter == 0");
+    if (params->return_map != 0u)
+        return na_fail(err, err_len, MPM_ERR_ARG, "return_map %u needs a handle (deferred plasticity pass)",
+                       params->return_map);
     if ((collider_words && !collider_data) || (n_nodes && !bvh_nodes))
         return na_fail(err, err_len, MPM_ERR_ARG, "null collider buffer");
     if ((size_t)num_indices > collider_words)

@@ -105,6 +105,8 @@ struct SceneDev {
     // dts = dt * 2^k with the same i32 result
     uint32_t fold;
     float rdts, dts;
+    uint32_t rmap;     // return map: 0 applyPlasticity, 1 SVD clamp (deferred pass only)
+    uint32_t rmap_pad;
 };
 static_assert(sizeof(SceneDev) % 8 == 0, "SceneDev must be 8-byte sized");
 

@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(128) k_plasticity_exact(Ctx c, PlastCtx pc) {
             warp_count(&pc.stats->fallback_domain, !dom);
             float Fe2[9], Fp2[9];
             for (int k = 0; k < 9; k++) { Fe2[k] = Fe[k]; Fp2[k] = Fp[k]; }
-            plasticity_exact(S.smin, S.smax, Fe2, Fp2);
+            plasticity_map(S.rmap, S.smin, S.smax, Fe2, Fp2);
             if (MODE == PLAST_COLLECT && dom && pc.pair_x && hash3(pid, step, 0xc011u) < pc.audit_threshold) {
                 uint32_t slot = atomicAdd(pc.pair_count, 1u);
                 if (slot < pc.pair_cap) {
@@ -264,10 +264,12 @@ __global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) 
         float Fe[9], Fp[9], x[12] = {0.f};
         bool dom = false;
         float smin = 0.f, smax = 0.f;
+        uint32_t rmap = 0u;
         if (valid) {
             const SceneDev& S = c.scenes[find_scene_p(c, pid)];
             smin = S.smin;
             smax = S.smax;
+            rmap = S.rmap;
             load_fe_fp(c.work_out, c.n_particles, slot, Fe, Fp);
             dom = mlp_features(Fe, Fp, S.dt, 1.0f - S.smin, x);
             if (!dom)
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) 
         if (!use || audit) {
             float Fe2[9], Fp2[9];
             for (int k = 0; k < 9; k++) { Fe2[k] = Fe[k]; Fp2[k] = Fp[k]; }
-            plasticity_exact(smin, smax, Fe2, Fp2);
+            plasticity_map(rmap, smin, smax, Fe2, Fp2);
             if (audit) {
                 float err = 0.f;
                 for (int k = 0; k < 9; k++) err = fmaxf(err, fabsf(Fn[k] - Fe2[k]));

@@ -50,6 +50,71 @@ __device__ __forceinline__ void plasticity_exact(float smin, float smax, float* 
     for (int i = 0; i < 9; i++) Fe[i] = Fn[i];
 }
 
+// The SVD return map (return_map 1): an option of this library, not the
+// reference's map.  One-sided Jacobi SVD (M. R. Hestenes, "Inversion of
+// matrices by biorthogonalization and related results", J. SIAM 6, 1958): the
+// column pairs (0,1), (0,2), (1,2) of A = Fe are rotated, SVD_SWEEPS sweeps,
+// until A V = U diag(sigma) with sigma_k = |a_k|.  If every sigma lies in
+// [smin, smax] nothing changes, else Fe' = sum_k (clamp(sigma_k) / sigma_k)
+// a_k v_k^T and Fp' = Fe'^-1 (Fe Fp).  The oracle's plasticity_svd performs
+// the same operations.  cert_elastic certifies this map too: it bounds the
+// singular values themselves.
+constexpr int SVD_SWEEPS = 4;
+__device__ __forceinline__ void jrot(float* x, float* y, float c, float sn) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const float xr = x[r], yr = y[r];
+        x[r] = fs(fm(c, xr), fm(sn, yr));
+        y[r] = fa(fm(sn, xr), fm(c, yr));
+    }
+}
+
+static __device__ __noinline__ void plasticity_svd(float smin, float smax, float* Fe, float* Fp) {
+    float a[9], v[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+#pragma unroll
+    for (int i = 0; i < 9; i++) a[i] = Fe[i];
+#pragma unroll 1
+    for (int sw = 0; sw < SVD_SWEEPS; sw++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int p = k == 2 ? 1 : 0, q = k == 0 ? 1 : 2;
+            float* ap = a + 3 * p;
+            float* aq = a + 3 * q;
+            const float al = dot3(ap, ap), be = dot3(aq, aq), ga = dot3(ap, aq);
+            if (ga == 0.f) continue;
+            const float ze = fd(fs(be, al), fm(2.f, ga));
+            const float t = fd(copysignf(1.f, ze), fa(fabsf(ze), __fsqrt_rn(ff(ze, ze, 1.f))));
+            const float c = fd(1.f, __fsqrt_rn(ff(t, t, 1.f)));
+            const float sn = fm(c, t);
+            jrot(ap, aq, c, sn);
+            jrot(v + 3 * p, v + 3 * q, c, sn);
+        }
+    float sg[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) sg[k] = __fsqrt_rn(dot3(a + 3 * k, a + 3 * k));
+    if (smin <= sg[0] && smin <= sg[1] && smin <= sg[2] && sg[0] <= smax && sg[1] <= smax && sg[2] <= smax) return;
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) w[k] = sg[k] > 0.f ? fd(fminf(fmaxf(sg[k], smin), smax), sg[k]) : 1.f;
+    float Fn[9], Fni[9], F[9];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            Fn[3 * j + r] = ff(fm(w[2], a[6 + r]), v[6 + j], ff(fm(w[1], a[3 + r]), v[3 + j], fm(fm(w[0], a[r]), v[j])));
+    inv3(Fn, Fni);
+    mul3(Fe, Fp, F);
+    mul3(Fni, F, Fp);
+#pragma unroll
+    for (int i = 0; i < 9; i++) Fe[i] = Fn[i];
+}
+
+// The return map a scene selects (MpmParams::return_map).
+__device__ __forceinline__ void plasticity_map(uint32_t rmap, float smin, float smax, float* Fe, float* Fp) {
+    if (rmap == 1u) plasticity_svd(smin, smax, Fe, Fp);
+    else plasticity_exact(smin, smax, Fe, Fp);
+}
+
 __device__ __forceinline__ bool cert_elastic(float smin, float smax, const float* Fe) {
     // C[i][j] = dot(column i, column j)
     float c00 = dot3(Fe, Fe), c11 = dot3(Fe + 3, Fe + 3), c22 = dot3(Fe + 6, Fe + 6);
