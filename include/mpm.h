@@ -116,8 +116,15 @@ int mpm_set_scene_range(MpmHandle* h, uint32_t scene, uint32_t first, uint32_t c
 int mpm_set_scene_count(MpmHandle* h, uint32_t n_scenes);
 
 /* ---- particles (GpuMpmBufferManager.ts:22-26) ---------------------- */
-/* Copies n 192-byte records into the library buffer (src on host or device). */
+/* Copies n 192-byte records into the library buffer (src on host or device;
+ * a host copy is enqueued on the handle's stream: asynchronous from pinned
+ * memory).  The library advances its own copy of the state with the records
+ * in tile order; mpm_get_particles (and mpm_particles_device_ptr, and every
+ * step call on a caller-bound buffer) restores the caller's order first. */
 int mpm_set_particles(MpmHandle* h, const void* src, uint32_t n, int src_is_device);
+/* dst_is_device: 0 host memory, the call waits for the copy; 1 device memory;
+ * 2 host memory, the copy is only enqueued on the handle's stream (dst must
+ * be pinned and is valid after mpm_sync or a stream synchronisation). */
 int mpm_get_particles(MpmHandle* h, void* dst, uint32_t n, int dst_is_device);
 /* Zero-copy: the step reads and writes the caller's device buffer of n records. */
 int mpm_bind_particles_device(MpmHandle* h, void* dptr, uint32_t n);

@@ -256,4 +256,11 @@ def test_device_upload_and_pointer(gpu, oracle_mod):
 
     recs = torch.as_tensor(_Raw(), device="cuda").clone()
     compare_states(recs.cpu().numpy().view(spec.particles.dtype), want)
+    # readback into pinned host memory without waiting (dst_is_device = 2)
+    assert g.step(1) == 0
+    _, want3 = run_oracle(oracle_mod, spec, n_steps=3)
+    pinned = torch.zeros(nbytes, dtype=torch.uint8, pin_memory=True)
+    assert lib.mpm_get_particles(g.buf.handle, C.c_void_p(pinned.data_ptr()), n, 2) == 0
+    assert g.buf.sync() == 0
+    compare_states(pinned.numpy().view(spec.particles.dtype), want3)
     g.close()

@@ -624,8 +624,8 @@ extern "C" int mpm_get_particles(MpmHandle* h, void* dst, uint32_t n, int dst_is
     int r = flush_records(h);
     if (r) return r;
     if (n) CK(h, cudaMemcpyAsync(dst, h->particles, (size_t)n * MPM_PARTICLE_BYTES,
-                                 dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
-    if (!dst_is_device) CK(h, cudaStreamSynchronize(h->stream));
+                                 dst_is_device == 1 ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    if (dst_is_device == 0) CK(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
 
