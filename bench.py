@@ -904,6 +904,35 @@ def results_table(local):
     return rows
 
 
+def step_case(args, local):
+    """The substep alone (the profiling case of the step's kernels): builds the
+    slab of --counts, runs --warmup then --steps PBMPM substeps through the
+    public API and prints the CUDA-event time per substep; no other leg."""
+    import torch
+
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module(PKG)
+    spec = build_scene(pkg, counts=args.counts)
+    n = spec.particles.shape[0]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    buf, pipe = _pipeline(pkg, spec, args.tile_edge, stream, local)
+    method = pkg.GpuSimulationMethodType.Pbmpm
+    for _ in range(args.warmup):
+        pipe.step(method, 1)
+    status = buf.sync()
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    for _ in range(args.steps):
+        pipe.step(method, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"case": "step", "particles": n, "tiles": buf.counts()[0], "ms_per_substep": ms,
+                      "value": n / (ms * 1e-3), "device_status": status}), flush=True)
+    buf.close()
+
+
 def mlp_case(local):
     """The network alone (the profiling case of its kernels): forward passes over
     1,048,576 random rows and one training epoch over 65,536 random pairs;
@@ -952,6 +981,8 @@ def main():
                     help="measure configs 0-2 against the f32 and f64 oracles (one JSON line per config)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the learned-plasticity and batched-scene legs (they run at N = 1 only)")
+    ap.add_argument("--step-only", action="store_true",
+                    help="run only warm-up + timed substeps of the slab (profiling case of the step's kernels)")
     ap.add_argument("--batched", action="store_true",
                     help="config 3 instead: 256 independent scenes sharded by scene over the ranks")
     ap.add_argument("--counts", default="256,64,256",
@@ -964,6 +995,9 @@ def main():
         return
     if args.results_table:
         results_table(dist_env()[2])
+        return
+    if args.step_only:
+        step_case(args, dist_env()[2])
         return
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()

@@ -864,7 +864,7 @@ static cudaError_t launch(MpmHandle* h, uint32_t kid, const Ctx& c, bool capturi
         pc.pair_cap = h->pair_cap;
         // INLINE with an SVD scene: the exact pass applies each scene's map
         const int pm = h->plast_mode == PLAST_INLINE ? PLAST_EXACT : h->plast_mode;
-        e = launch_plasticity(pm, c, pc, h->n_sms * (pm == PLAST_LEARNED ? 4 : 8), h->stream);
+        e = launch_plasticity(pm, c, pc, h->n_sms * (pm == PLAST_LEARNED ? (int)MLP_CTAS_PER_SM : 8), h->stream);
     } else {
         e = launch_e(h->tile_edge, kid, c, h->stream, grid, 0, 0, nullptr);
     }
@@ -1476,7 +1476,7 @@ extern "C" int mpm_mlp_forward(MpmMlp* m, const float* x_dev, uint32_t n, float*
     if (!m || (n && (!x_dev || !y_dev))) return MPM_ERR_ARG;
     if (n == 0) return MPM_OK;
     cudaSetDevice(m->device);
-    int grid = (int)std::min<uint32_t>((n + 127u) / 128u, (uint32_t)m->n_sms * 4u);
+    int grid = (int)std::min<uint32_t>((n + 127u) / 128u, (uint32_t)m->n_sms * MLP_CTAS_PER_SM);
     MCK(m, launch_mlp_forward(m->params, x_dev, n, y_dev, m->err, grid, m->stream));
     MCK(m, cudaStreamSynchronize(m->stream));
     return mlp_check_err(m);

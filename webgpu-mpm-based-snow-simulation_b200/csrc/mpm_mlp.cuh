@@ -21,6 +21,9 @@ static_assert(NPARAM == 9867, "parameter count");
 
 // plasticity pass modes (after integrate; mode 0 keeps the exact map inline)
 constexpr int PLAST_INLINE = 0, PLAST_EXACT = 1, PLAST_COLLECT = 2, PLAST_LEARNED = 3;
+// resident CTAs per SM of the inference kernels (36 KB of shared memory and
+// 64 tensor-memory columns each): one CTA's epilogue runs while another's MMAs do
+constexpr unsigned MLP_CTAS_PER_SM = 6;
 
 struct PlastStats {
     unsigned long long candidates;          // particles the strain-bound check did not clear
