@@ -130,7 +130,6 @@ struct MpmHandle {
     uint32_t* chunk_nst = nullptr;
     uint32_t* chunk_np = nullptr;
     int4* tiles[3] = {nullptr, nullptr, nullptr};   // first transfer, then the PBMPM iterations' ping-pong
-    float* tile_rm = nullptr;     // max_tiles x (E+2)^3 reciprocal cell masses
     int32_t* st_nbr = nullptr;    // max_tiles x 27 neighbour indices
     uint32_t* tile_order = nullptr;  // max_tiles: the tile kernels' claim order
     // deferred / learned plasticity
@@ -363,7 +362,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
     for (auto e : h->event_pool) cudaEventDestroy(e);
     void* bufs[] = {h->work[0], h->work[1], h->ids[0], h->ids[1], h->sorted, h->bin_slot, h->bin_rank, h->keys, h->slot_count, h->slot_off,
                     h->slot_st, h->st_key, h->st_slot, h->st_begin, h->st_count, h->chunk_nst, h->chunk_np,
-                    h->tiles[0], h->tiles[1], h->tiles[2], h->tile_rm, h->d_scenes, h->d_scene_first, h->counters,
+                    h->tiles[0], h->tiles[1], h->tiles[2], h->d_scenes, h->d_scene_first, h->counters,
                     h->iter_rec, h->st_nbr, h->tile_order,
                     h->plast_list, h->d_stats, h->d_pair_count};
     for (void* b : bufs)
@@ -413,11 +412,9 @@ static int alloc_tiles(MpmHandle* h, uint32_t n) {
         if (h->tiles[i]) { cudaFree(h->tiles[i]); h->tiles[i] = nullptr; }
     if (h->st_nbr) { cudaFree(h->st_nbr); h->st_nbr = nullptr; }
     if (h->tile_order) { cudaFree(h->tile_order); h->tile_order = nullptr; }
-    if (h->tile_rm) { cudaFree(h->tile_rm); h->tile_rm = nullptr; }
     size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     h->max_tiles = n;
     for (int i = 0; i < 3; i++) CK(h, cudaMalloc(&h->tiles[i], (size_t)n * NC * 16));
-    CK(h, cudaMalloc(&h->tile_rm, (size_t)n * NC * 4));
     CK(h, cudaMalloc(&h->st_nbr, (size_t)n * 27 * 4));
     CK(h, cudaMalloc(&h->tile_order, (size_t)n * 4));
     destroy_graphs(h);
@@ -802,7 +799,6 @@ static Ctx make_ctx(MpmHandle* h, int cur) {
     c.st_nbr = h->st_nbr;
     c.tile_order = h->tile_order;
     c.order_mode = h->order_mode;
-    c.tile_rm = h->tile_rm;
     c.plast_list = h->plast_list;
     c.plast_defer = (h->plast_mode != PLAST_INLINE || h->svd_any) ? 1u : 0u;
     c.scenes = h->d_scenes;
@@ -1634,8 +1630,7 @@ constexpr size_t NA_TILES0 = NA_CHUNK_NP + na_round(NA_H / COMPACT_CHUNK * 4);  
 constexpr size_t NA_TILES1 = NA_TILES0 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);
 constexpr size_t NA_ITER_REC = NA_TILES1 + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 16);  // PBMPM records
 constexpr size_t NA_ST_NBR = NA_ITER_REC + na_round(NA_P * IR_PLANES * 16);  // tile neighbour table
-constexpr size_t NA_RM = NA_ST_NBR + na_round(MPM_NOALLOC_MAX_TILES * 27 * 4);   // reciprocal cell masses
-constexpr size_t NA_SCENE = NA_RM + na_round(MPM_NOALLOC_MAX_TILES * NA_NC * 4);
+constexpr size_t NA_SCENE = NA_ST_NBR + na_round(MPM_NOALLOC_MAX_TILES * 27 * 4);
 constexpr size_t NA_SCENE_FIRST = NA_SCENE + na_round(sizeof(SceneDev));
 constexpr size_t NA_COUNTERS = NA_SCENE_FIRST + na_round(2 * 4);
 constexpr size_t NA_BYTES = NA_COUNTERS + na_round(sizeof(Counters));
@@ -1775,7 +1770,6 @@ extern "C" int mpm_step_noalloc(int device, void* stream, void* particles, uint3
     c.tiles_b = tiles[0];
     c.iter_rec = (float4*)(b + NA_ITER_REC);
     c.st_nbr = (int32_t*)(b + NA_ST_NBR);
-    c.tile_rm = (float*)(b + NA_RM);
     c.scenes = (const SceneDev*)(b + NA_SCENE);
     c.scene_first = (const uint32_t*)(b + NA_SCENE_FIRST);
     c.counters = (Counters*)(b + NA_COUNTERS);

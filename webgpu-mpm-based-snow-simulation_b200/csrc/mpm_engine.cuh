@@ -18,9 +18,9 @@
 //   st_key/st_slot/st_begin/st_count   per compact tile
 //   tiles[3]    max_tiles x (E+2)^3 x int4   per-tile halo sums
 //               (mass, momentum x, y, z) in the reference i32 fixed point;
-//               the PBMPM iterations write momentum only (mass field 0)
-//   tile_rm     max_tiles x (E+2)^3 f32      reciprocal cell masses of the
-//               substep, formed by its first PBMPM iteration
+//               the PBMPM iterations write the cell's reciprocal mass of the
+//               substep (f32 bits, formed by the first iteration) in place of
+//               the mass, and their momentum sums
 //   iter_rec    IR_PLANES x N float4         PBMPM iteration records (below)
 //   st_nbr      max_tiles x 27 i32           compact index of each tile's 27
 //                                            neighbours (d = 9(dz+1) + 3(dy+1) + dx+1),
@@ -164,10 +164,9 @@ struct Ctx {
     uint32_t order_rev;       // this launch claims tile_order from its end (alternates per launch)
     uint32_t order_mode;      // tile claim order: 0 automatic, 1 compact index order, 4 / 5 Morton
                               // buckets of 4 / 5 bits per axis (schedule knob of the autotuner)
-    float* tile_rm;           // per tile (E+2)^3 reciprocal cell masses of the substep (PBMPM iterations)
     const int4* tiles_m;      // readback only: tiles holding the substep's mass sums (nullptr: tiles_b)
-    uint32_t iter_first;      // this PBMPM iteration forms and stores the reciprocal masses
-    uint32_t g2p_rm;          // the final PBMPM G2P reads the stored reciprocal masses
+    uint32_t iter_first;      // this PBMPM iteration forms the reciprocal masses from the mass sums
+    uint32_t g2p_rm;          // the final PBMPM G2P reads the reciprocal masses from the halo records
     uint32_t* plast_list;     // deferred plasticity: work_out slots the strain-bound check did not clear
     uint32_t plast_defer;     // 0: exact return map inside integrate; 1: deferred to the plasticity pass
     const SceneDev* scenes;

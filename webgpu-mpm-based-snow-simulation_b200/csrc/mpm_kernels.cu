@@ -944,25 +944,22 @@ struct HaloCopy {
     uint32_t parity;
 };
 
-// Thread 0 issues the bulk copies of tile st's own (E+2)^3 sums (and of its
-// stored reciprocal masses when rm_dst is given) into shared memory; they
-// complete on hc's mbarrier.
+// Thread 0 issues the bulk copies of tile st's own (E+2)^3 sums into shared
+// memory; they complete on hc's mbarrier.
 template <int E>
-__device__ __forceinline__ void halo_issue(const int4* tiles, uint32_t st, int4* cell, HaloCopy& hc,
-                                           const float* rm_src, float* rm_dst) {
+__device__ __forceinline__ void halo_issue(const int4* tiles, uint32_t st, int4* cell, HaloCopy& hc) {
     constexpr int H = E + 2, NC = H * H * H;
     if (threadIdx.x == 0) {
         const int4* own = tiles + (size_t)st * NC;
         // the previous tile's shared-memory reads (generic proxy) come before these writes
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(hc.mbar, (uint32_t)(NC * 16 + (rm_dst ? NC * 4 : 0)));
+        mbar_expect_tx(hc.mbar, (uint32_t)(NC * 16));
         constexpr uint32_t CH = (NC * 16) / 4 / 16 * 16;   // four chunks, 16-byte multiples
         bulk_g2s(cell, own, CH, hc.mbar);
         bulk_g2s(reinterpret_cast<char*>(cell) + CH, reinterpret_cast<const char*>(own) + CH, CH, hc.mbar);
         bulk_g2s(reinterpret_cast<char*>(cell) + 2 * CH, reinterpret_cast<const char*>(own) + 2 * CH, CH, hc.mbar);
         bulk_g2s(reinterpret_cast<char*>(cell) + 3 * CH, reinterpret_cast<const char*>(own) + 3 * CH,
                  (uint32_t)(NC * 16) - 3 * CH, hc.mbar);
-        if (rm_dst) bulk_g2s(rm_dst, rm_src, (uint32_t)(NC * 4), hc.mbar);
     }
 }
 
@@ -971,20 +968,19 @@ __device__ __forceinline__ void halo_issue(const int4* tiles, uint32_t st, int4*
 // of the compile-time halo table, loaded into registers in batches of U per
 // thread and added with shared i32 atomics).  The first batch of neighbour
 // loads is issued before the wait for the bulk copy, so both latencies
-// overlap.  rm_src / rm_dst (optional): the tile's stored reciprocal masses,
-// brought in by the same bulk copy.  MASS = false adds only the momentum
-// components (the mass field of the result is then undefined).  Returns false
-// (on every thread) when the copy wait ran out; the caller then stops.
-// PRE = true: the caller issued the own-halo copies earlier (halo_issue).
+// overlap.  MASS = false adds only the momentum components: the mass field
+// of the result keeps the tile's own record (in the PBMPM iterations' halo
+// records, the reciprocal cell mass).  Returns false (on every thread) when
+// the copy wait ran out; the caller then stops.  PRE = true: the caller issued
+// the own-halo copies earlier (halo_issue).
 template <int E, int BS, bool MASS = true, bool PRE = false>
-__device__ __forceinline__ bool assemble_sums(const int4* tiles, const int* nbr, int4* cell, HaloCopy& hc,
-                                              const float* rm_src = nullptr, float* rm_dst = nullptr) {
+__device__ __forceinline__ bool assemble_sums(const int4* tiles, const int* nbr, int4* cell, HaloCopy& hc) {
     constexpr int H = E + 2, NC = H * H * H;
     constexpr int NE = HaloEntries<E>::N;
     constexpr int PER = (NE + BS - 1) / BS;      // entries per thread
     constexpr int U = PER <= 10 ? PER : 8;       // entries per register batch
     const uint32_t* tab = halo_table<E>();
-    if (!PRE) halo_issue<E>(tiles, (uint32_t)nbr[13], cell, hc, rm_src, rm_dst);
+    if (!PRE) halo_issue<E>(tiles, (uint32_t)nbr[13], cell, hc);
     int4 v[U];
     int jd[U];
     auto fetch = [&](int base) {
@@ -1047,24 +1043,17 @@ __device__ __forceinline__ float4 cell_velocity_rm(const SceneDev& S, int4 s, fl
 // (assemble_sums), then each sum turned into the velocity in place.  RM
 // selects where the cell masses come from: 0, the assembled mass sums (the
 // reference path, explicit grid update included); 1, the same, and the
-// reciprocal masses are also stored to rm_tile for later passes of the
-// substep; 2, the reciprocal masses stored by such a pass (the halo sums then
-// carry momentum only), brought into rm_s by the halo's bulk copy when rm_s
-// is given, else loaded after the assembly into the unused mass field.
-// Returns false (on every thread) when the halo copy wait ran out.
+// reciprocal masses RN(1/m) are kept in rm_s for the tile's flush; 2, the
+// reciprocal masses carried in the mass word of the tile's own halo record
+// (written there by the previous PBMPM iteration's flush; the halo sums then
+// carry momentum only), also kept in rm_s when it is given.  Returns false (on
+// every thread) when the halo copy wait ran out.
 template <int E, int BS, bool PB, int RM = 0, bool PRE = false>
 __device__ __forceinline__ bool assemble_velocity_tile(const int4* tiles, const SceneDev& S, const TileCtx<E>& T,
                                                        const int* nbr, int4* cell, HaloCopy& hc,
-                                                       float* rm_tile = nullptr, float* rm_s = nullptr) {
+                                                       float* rm_s = nullptr) {
     constexpr int H = E + 2, NC = H * H * H;
-    const bool rm_bulk = RM == 2 && rm_s != nullptr;
-    if (!assemble_sums<E, BS, RM != 2, PRE>(tiles, nbr, cell, hc, rm_bulk ? rm_tile : nullptr,
-                                            rm_bulk ? rm_s : nullptr))
-        return false;
-    if (RM == 2 && !rm_bulk) {
-#pragma unroll 8
-        for (int j = threadIdx.x; j < NC; j += BS) cell[j].x = __float_as_int(__ldg(rm_tile + j));
-    }
+    if (!assemble_sums<E, BS, RM != 2, PRE>(tiles, nbr, cell, hc)) return false;
     __syncthreads();
     // batches of CB cells per thread: all loads, then all conversions, then
     // all stores, so the cells' dependency chains overlap
@@ -1076,7 +1065,7 @@ __device__ __forceinline__ bool assemble_velocity_tile(const int4* tiles, const 
         for (int u = 0; u < CB; u++) {
             int j = j0 + u * BS;
             sm[u] = j < NC ? cell[j] : make_int4(0, 0, 0, 0);
-            rmu[u] = (RM == 2 && j < NC) ? (rm_bulk ? rm_s[j] : __int_as_float(sm[u].x)) : 0.0f;
+            rmu[u] = (RM == 2 && j < NC) ? __int_as_float(sm[u].x) : 0.0f;
         }
         float4 v[CB];
 #pragma unroll
@@ -1090,10 +1079,10 @@ __device__ __forceinline__ bool assemble_velocity_tile(const int4* tiles, const 
                 float rm;
                 if (RM == 1) {
                     rm = mass_recip(S, sm[u].x, gc);
-                    if (j < NC) rm_tile[j] = rm;
                 } else {
                     rm = rmu[u];
                 }
+                if (rm_s != nullptr && j < NC) rm_s[j] = rm;
                 v[u] = cell_velocity_rm(S, sm[u], rm, gc);
             }
         }
@@ -1379,12 +1368,15 @@ __device__ __forceinline__ void zero_mom(uint32_t* acc) {
     for (int j = threadIdx.x; j < 3 * NC / 4; j += blockDim.x) a4[j] = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// halo record of a PBMPM iteration: the cell's reciprocal mass RN(1/m) of the
+// substep (the same in every tile that covers the cell) in the mass word,
+// this tile's momentum sums in the other three
 template <int E>
-__device__ __forceinline__ void flush_mom(const uint32_t* acc, int4* dst) {
+__device__ __forceinline__ void flush_mom(const uint32_t* acc, const float* rm_s, int4* dst) {
     constexpr int H = E + 2, NC = H * H * H;
 #pragma unroll 4
     for (int j = threadIdx.x; j < NC; j += blockDim.x)
-        dst[j] = make_int4(0, (int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j]);
+        dst[j] = make_int4(__float_as_int(rm_s[j]), (int)acc[j], (int)acc[NC + j], (int)acc[2 * NC + j]);
 }
 
 template <int E>
@@ -1653,8 +1645,7 @@ __global__ void __launch_bounds__(BS) k_g2p_integrate(Ctx c) {
         tile_begin<E>(c, st, S, T, cur_scene);
         load_neighbors(c, st, nbr);
         __syncthreads();
-        constexpr int NCT = (E + 2) * (E + 2) * (E + 2);
-        if (!assemble_velocity_tile<E, BS, PB, RM>(c.tiles_b, S, T, nbr, cell, hc, c.tile_rm + (size_t)st * NCT)) {
+        if (!assemble_velocity_tile<E, BS, PB, RM>(c.tiles_b, S, T, nbr, cell, hc)) {
             copy_wait_failed(c, hc);
             tiles_done(c);
             return;
@@ -1751,9 +1742,11 @@ __global__ void __launch_bounds__(BS) k_pbmpm_first(Ctx c) {
 // all from the iteration records (contiguous in tile order).  Positions and
 // masses are fixed within a substep, so the cell masses are the first
 // transfer's: the first iteration (FIRST) forms their reciprocals from the
-// mass sums and stores them; later iterations read them back, and every
-// iteration accumulates and writes momentum only.  Shared memory: the halo
-// sums / velocities (16 B per cell) and three momentum planes (12 B per cell).
+// mass sums; every iteration accumulates momentum only and writes, per halo
+// cell, the reciprocal mass and its momentum sums, so the next pass reads the
+// reciprocal masses with its own halo record.  Shared memory: the halo sums /
+// velocities (16 B per cell), three momentum planes (12 B per cell) and the
+// reciprocal masses (4 B per cell).
 template <int E, int BS, bool FIRST>
 __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     constexpr int H = E + 2, NC = H * H * H;
@@ -1761,7 +1754,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     int4* cell = reinterpret_cast<int4*>(smem_raw);
     const float4* vel = reinterpret_cast<const float4*>(smem_raw);
     uint32_t* acc = reinterpret_cast<uint32_t*>(smem_raw + NC);
-    float* rm_s = reinterpret_cast<float*>(acc + 3 * NC);   // stored reciprocal masses (later iterations)
+    float* rm_s = reinterpret_cast<float*>(acc + 3 * NC);   // reciprocal cell masses, for the flush
     __shared__ SceneDev S;
     __shared__ int nbr[27];
     __shared__ uint64_t mbar;
@@ -1775,8 +1768,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
     // particles are done, so they overlap that tile's flush
     const uint32_t st0 = tile_at(c, blockIdx.x, n_st);
     if (st0 < n_st)
-        halo_issue<E>(c.tiles_b, st0, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)st0 * NC,
-                      FIRST ? nullptr : rm_s);
+        halo_issue<E>(c.tiles_b, st0, cell, hc);
     for (uint32_t st = st0; st < n_st; st = s_next) {
         TileCtx<E> T;
         tile_begin<E>(c, st, S, T, cur_scene);
@@ -1784,8 +1776,7 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
         zero_mom<E>(acc);
         __syncthreads();
         if (!assemble_velocity_tile<E, BS, true, FIRST ? 1 : 2, true>(c.tiles_b, S, T, nbr, cell, hc,
-                                                                     c.tile_rm + (size_t)st * NC,
-                                                                     FIRST ? nullptr : rm_s)) {
+                                                                     rm_s)) {
             copy_wait_failed(c, hc);
             tiles_done(c);
             return;
@@ -1808,10 +1799,9 @@ __global__ void __launch_bounds__(BS) k_pbmpm_iter(Ctx c) {
             const uint32_t nx = claim_tile(c, n_st);
             s_next = nx;
             if (nx < n_st)
-                halo_issue<E>(c.tiles_b, nx, cell, hc, FIRST ? nullptr : c.tile_rm + (size_t)nx * NC,
-                              FIRST ? nullptr : rm_s);
+                halo_issue<E>(c.tiles_b, nx, cell, hc);
         }
-        flush_mom<E>(acc, c.tiles_a + (size_t)st * NC);
+        flush_mom<E>(acc, rm_s, c.tiles_a + (size_t)st * NC);
         __syncthreads();
     }
     tiles_done(c);
