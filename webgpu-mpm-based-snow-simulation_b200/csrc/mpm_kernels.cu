@@ -523,9 +523,11 @@ __device__ __forceinline__ void defer_plasticity(const Ctx& c, uint32_t pid) {
     c.plast_list[base + (uint32_t)__popc(m & lanemask_lt())] = pid;
 }
 
-// integrateParticles (integrateParticles.wgsl:14-72).  With deferred
-// plasticity the record keeps the trial Fe; particles the strain-bound check
-// does not clear are listed for the plasticity pass (exact or learned).
+// integrateParticles (integrateParticles.wgsl:14-72).  The return map runs
+// only for particles the strain-bound check does not clear (for the others it
+// returns Fe and Fp unchanged, bit for bit).  With deferred plasticity the
+// record keeps the trial Fe and those particles are listed for the plasticity
+// pass (exact or learned).
 __device__ __forceinline__ void integrate(const Ctx& c, const SceneDev& S, PState& p, uint32_t pid) {
     Counters* ctr = c.counters;
 #pragma unroll
@@ -534,9 +536,10 @@ __device__ __forceinline__ void integrate(const Ctx& c, const SceneDev& S, PStat
 #pragma unroll
     for (int i = 0; i < 9; i++) IpD[i] = fa((i == 0 || i == 4 || i == 8) ? 1.0f : 0.0f, p.D[i]);
     mul3(IpD, p.Fe, p.Fe);
+    const bool certified = cert_elastic(S.smin, S.smax, p.Fe);
     if (c.plast_defer) {
-        if (!cert_elastic(S.smin, S.smax, p.Fe)) defer_plasticity(c, pid);
-    } else {
+        if (!certified) defer_plasticity(c, pid);
+    } else if (!certified) {
         plasticity(S, p.Fe, p.Fp);
     }
 #pragma unroll

@@ -140,10 +140,10 @@ __device__ bool tile_forward(InfSmem& sm, uint32_t tmem, uint32_t& phase, const 
     const float* bl[3] = {sm.b1, sm.b2, sm.b3};
     for (int layer = 0; layer < 3; layer++) {
         // hidden activation of the layer just computed -> next A operand
-        for (int c0 = 0; c0 < HID; c0 += 16) {
-            float z[16];
-            tc::tmem_ld16(tc::tmem_addr(tmem, warp * 32u, (uint32_t)c0), z);
-            for (int h = 0; h < 2; h++) {
+        for (int c0 = 0; c0 < HID; c0 += 32) {
+            float z[32];
+            tc::tmem_ld32(tc::tmem_addr(tmem, warp * 32u, (uint32_t)c0), z);
+            for (int h = 0; h < 4; h++) {
                 for (int i = 0; i < 8; i++) v[i] = silu(z[h * 8 + i] + bl[layer][c0 + h * 8 + i]);
                 st_row8(sm.a, r, (uint32_t)(c0 + h * 8), ROWS, v);
             }
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(128) k_plasticity_exact(Ctx c, PlastCtx pc) {
 }
 
 // learned surrogate with gating, audit and exact fallback, 128 particles per tile
-__global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) {
+__global__ void __launch_bounds__(128, MLP_CTAS_PER_SM) k_plasticity_learned(Ctx c, PlastCtx pc) {
     const uint32_t count = c.counters->n_plast;
     __shared__ InfSmem sm;
     const uint32_t warp = threadIdx.x >> 5;
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(128) k_plasticity_learned(Ctx c, PlastCtx pc) 
 }
 
 // raw network on device arrays: x [n][12] -> y [n][11]
-__global__ void __launch_bounds__(128) k_mlp_forward(const float* P, const float* xin, uint32_t n, float* yout,
+__global__ void __launch_bounds__(128, MLP_CTAS_PER_SM) k_mlp_forward(const float* P, const float* xin, uint32_t n, float* yout,
                                                      uint32_t* err) {
     __shared__ InfSmem sm;
     const uint32_t warp = threadIdx.x >> 5;

@@ -111,6 +111,33 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 consecutive f32 columns as two loads in flight and one wait; the wait
+// names the destination registers, so no use of them moves ahead of it
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+            : "=r"(r[16 * h + 0]), "=r"(r[16 * h + 1]), "=r"(r[16 * h + 2]), "=r"(r[16 * h + 3]),
+              "=r"(r[16 * h + 4]), "=r"(r[16 * h + 5]), "=r"(r[16 * h + 6]), "=r"(r[16 * h + 7]),
+              "=r"(r[16 * h + 8]), "=r"(r[16 * h + 9]), "=r"(r[16 * h + 10]), "=r"(r[16 * h + 11]),
+              "=r"(r[16 * h + 12]), "=r"(r[16 * h + 13]), "=r"(r[16 * h + 14]), "=r"(r[16 * h + 15])
+            : "r"(taddr + 16u * (uint32_t)h)
+            : "memory");
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+                     : "+r"(r[16 * h + 0]), "+r"(r[16 * h + 1]), "+r"(r[16 * h + 2]), "+r"(r[16 * h + 3]),
+                       "+r"(r[16 * h + 4]), "+r"(r[16 * h + 5]), "+r"(r[16 * h + 6]), "+r"(r[16 * h + 7]),
+                       "+r"(r[16 * h + 8]), "+r"(r[16 * h + 9]), "+r"(r[16 * h + 10]), "+r"(r[16 * h + 11]),
+                       "+r"(r[16 * h + 12]), "+r"(r[16 * h + 13]), "+r"(r[16 * h + 14]), "+r"(r[16 * h + 15])
+                     :
+                     : "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ uint32_t tmem_addr(uint32_t base, uint32_t lane, uint32_t col) {
     return base + (lane << 16) + col;
 }
