@@ -33,6 +33,8 @@ PKG = "webgpu-mpm-based-snow-simulation_b200"
 METRIC = "particle-substeps/s at 4M (plain vs surrogate, agg err<=1e-3); P2G/G2P HBM GB/s"
 # learned plasticity: predicted-error threshold above which the exact map is used
 SURROGATE_UNC_THRESHOLD = 0.05
+# independent particle states in flight in the end-to-end measurement
+E2E_STATES = 3
 WORKLOAD = "c2_large_pbmpm: 4,194,304-particle snow slab on 130,050-tri fBm terrain, 512^3 sparse grid, PBMPM x6, dt 5e-5"
 
 
@@ -389,13 +391,13 @@ def gpu_run(args, rank, world, local):
     # ---- end to end through the public API with host buffers.  Each step
     # uploads a state's 192-byte records from pinned host memory
     # (mpm_set_particles), advances it one substep and reads the records back
-    # (mpm_get_particles).  Two states on two streams take turns, so one
-    # state's upload overlaps the other's readback and substep (PCIe copies
-    # run both directions at once); the serial chain of one state is timed
-    # beside it.
+    # (mpm_get_particles).  E2E_STATES states on their own streams take turns,
+    # so one state's upload overlaps the others' readbacks and substeps (PCIe
+    # copies run both directions at once); the serial chain of one state is
+    # timed beside it.
     e2e_steps = max(3, min(args.steps, 10))
     hosts, states = [], []
-    for k in range(2):
+    for k in range(E2E_STATES):
         host = torch.empty(n * 192, dtype=torch.uint8, pin_memory=True)
         host.numpy()[:] = np.frombuffer(spec.particles.tobytes(), np.uint8)
         hosts.append(host)
@@ -417,14 +419,14 @@ def gpu_run(args, rank, world, local):
         pp.step(method, 1)
         pkg._lib.check(lib.mpm_get_particles(b.handle, hp, n, 0 if wait else 2), b.handle)
 
-    e2e_issue(0, True)
-    e2e_issue(1, True)
+    for k in range(E2E_STATES):
+        e2e_issue(k, True)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        e2e_issue(0, False)
-        e2e_issue(1, False)
+        for k in range(E2E_STATES):
+            e2e_issue(k, False)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -432,14 +434,15 @@ def gpu_run(args, rank, world, local):
         e2e_issue(0, True)
     torch.cuda.synchronize()
     e2e_serial_s = time.perf_counter() - t0
-    states[1][0].close()
+    for b_, _, _ in states[1:]:
+        b_.close()
     del hosts, states
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([e2e_s, e2e_serial_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s, e2e_serial_s = (float(v) for v in t.tolist())
-    e2e_rate = world * n * 2 * e2e_steps / e2e_s
+    e2e_rate = world * n * E2E_STATES * e2e_steps / e2e_s
     e2e_serial = world * n * e2e_steps / e2e_serial_s
 
     launches_per_step = sum(v["launches_per_step"] for v in kernels.values())
@@ -466,7 +469,7 @@ def gpu_run(args, rank, world, local):
         "splats": splats,
         "kernels": {k: round(v["ms_per_launch"], 4) for k, v in kernels.items()},
         "e2e": {"value": e2e_rate, "unit": "particle-substeps/s", "h2d_bytes_per_step": n * 192,
-                "d2h_bytes_per_step": n * 192, "states_in_flight": 2, "serial_one_state": e2e_serial},
+                "d2h_bytes_per_step": n * 192, "states_in_flight": E2E_STATES, "serial_one_state": e2e_serial},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
         "device_status": status,
