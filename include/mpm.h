@@ -364,8 +364,9 @@ int mpm_get_plasticity_stats(MpmHandle* h, MpmPlasticityStats* out, int reset);
  * pool), or a real-time frame loop that must not pay cudaMalloc's implicit
  * device-wide synchronisation.  The caller passes its inputs and outputs
  * (particle records, collider arrays: device pointers on `device`); every
- * intermediate buffer of the substep (particle bins, tile hash table, grid
- * tile sums) lives in one static device array of MPM_NOALLOC_SCRATCH_BYTES
+ * intermediate buffer of the substep (the tile-ordered particle state,
+ * particle bins, tile hash table, grid tile sums) lives in one static device
+ * array of MPM_NOALLOC_SCRATCH_BYTES
  * that each GPU loading the library holds until the process exits.  The
  * call allocates nothing: no cudaMalloc, no cudaFree, no allocating library
  * routine.
