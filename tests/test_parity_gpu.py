@@ -9,7 +9,7 @@ test states a tolerance it is the relative bound 1e-5 on single-step fields.
 import numpy as np
 import pytest
 
-from helpers import GpuScene, bits_equal, compare_states, run_oracle
+from helpers import GpuScene, bits_equal, compare_states, make_params, run_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -271,3 +271,34 @@ def test_device_upload_and_pointer(gpu, oracle_mod):
     assert g.buf.sync() == 0
     compare_states(pinned.numpy().view(spec.particles.dtype), want3)
     g.close()
+
+
+@pytest.mark.parametrize("max_tiles,hash_capacity,bit", [(64, 0, 0x2), (8192, 4096, 0x1)])
+def test_capacity_overflow_keeps_every_particle(gpu, max_tiles, hash_capacity, bit):
+    """When tiles do not fit the tile storage (status 0x2) or the tile hash
+    table is full (0x1), the particles no tile kernel advances are carried
+    over unchanged: after the step every particle is still present once, at
+    its own caller index (masses, which a substep never changes, are all
+    distinct here), and the unadvanced ones keep their records bit for bit."""
+    spec = _scene(gpu, kind="explicit", res=256, n_side=20)
+    n = spec.particles.shape[0]
+    rng = np.random.default_rng(41)
+    spec.particles["pos"] = rng.uniform(0.05, 0.95, size=(n, 3)).astype(np.float32)
+    spec.particles["mass"] = (np.float32(1e-6) * (1.0 + np.arange(n) / n)).astype(np.float32)
+    buf = gpu.GpuMpmBufferManager(n_particles=n, tile_edge=8, max_tiles=max_tiles, hash_capacity=hash_capacity)
+    buf.write_particles(spec.particles)
+    pipe = gpu.GpuMpmPipelineManager(mpm_manager=buf, uniforms_manager=spec.uniforms,
+                                     params=make_params(gpu, spec.params))
+    pipe.add_explicit_mpm_dispatches(n_particles=n)
+    with pytest.raises(gpu.MpmError) as ei:
+        buf.sync()
+    assert ei.value.status & bit, ei.value.status
+    gpu.load().mpm_clear_status(buf.handle)
+    got = buf.read_particles()
+    assert np.array_equal(got["mass"].view(np.uint32), spec.particles["mass"].view(np.uint32))
+    same = np.all(got["pos"] == spec.particles["pos"], axis=1)
+    assert 0 < same.sum() < n, same.sum()
+    kept = got[same]
+    for f in ("vel", "Fe", "Fp", "dxp", "D"):
+        assert np.array_equal(kept[f].view(np.uint32), spec.particles[same][f].view(np.uint32)), f
+    buf.close()
