@@ -126,8 +126,12 @@ int mpm_set_particles(MpmHandle* h, const void* src, uint32_t n, int src_is_devi
  * 2 host memory, the copy is only enqueued on the handle's stream (dst must
  * be pinned and is valid after mpm_sync or a stream synchronisation). */
 int mpm_get_particles(MpmHandle* h, void* dst, uint32_t n, int dst_is_device);
-/* Zero-copy: the step reads and writes the caller's device buffer of n records. */
+/* Zero-copy: the caller's device buffer of n records (16-byte aligned) is the
+ * library's record buffer; every step call leaves it holding the advanced
+ * records in the caller's order (enqueued on the handle's stream). */
 int mpm_bind_particles_device(MpmHandle* h, void* dptr, uint32_t n);
+/* The device record buffer in the caller's order, brought up to date on the
+ * handle's stream first (read it after mpm_sync); NULL on failure. */
 void* mpm_particles_device_ptr(MpmHandle* h);
 
 /* ---- collider (GpuColliderBufferManager.ts:61-220) ------------------ */
