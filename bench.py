@@ -797,6 +797,33 @@ def batched_sharded(args, rank, world, local):
     }
 
 
+def f64_leg(pkg, args, local, stream, steps=3):
+    """The full workload (config 2 at 4,194,304 particles) against the f64
+    oracle: the GPU state after `steps` substeps from the initial records and
+    the f64 oracle's after the same substeps (the f64 oracle is the error
+    reference only; it runs on the host cores, outside any timed region)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the f64 error reference
+
+    spec = build_scene(pkg, counts=args.counts)
+    buf, pipe = _pipeline(pkg, spec, args.tile_edge, stream, local)
+    pipe.step(pkg.GpuSimulationMethodType.Pbmpm, steps)
+    status = buf.sync()
+    rec = buf.read_particles()
+    buf.close()
+    oracle.lib().orf_set_threads(os.cpu_count() or 1)
+    o = oracle.Oracle(spec.particles.shape[0], max_blocks=600000, hash_size=2000003, fp64=True)
+    o.set_collider(*spec.mesh)
+    p64 = oracle.to_fp64(spec.particles.copy())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(spec.uniforms.bytes(), spec.params, p64, 1)
+    oracle_s = time.perf_counter() - t0
+    o.close()
+    return {"particles": int(spec.particles.shape[0]), "substeps": steps, "device_status": status,
+            "agg_rel_err_vs_f64": _agg_rel_err(_agg(rec), _agg_any(p64)), "f64_oracle_s": round(oracle_s, 1)}
+
+
 def _agg_any(rec):
     """_agg for 192-byte records or the f64 oracle's records."""
     import numpy as np
@@ -1065,6 +1092,7 @@ def main():
         stream = torch.cuda.current_stream()
         out["surrogate"] = surrogate_leg(importlib.import_module(PKG), args, local, stream)
         out["batched"] = batched_leg(importlib.import_module(PKG), args, local, stream)
+        out["full_size_vs_f64"] = f64_leg(importlib.import_module(PKG), args, local, stream)
     if rank == 0:
         rate, cores, sample, _ = cpu_reference(args.cpu_steps, 1, args.counts)
         out["cpu_baseline"] = {"value": rate, "unit": "particle-substeps/s", "cores": cores, "kind": "port",
