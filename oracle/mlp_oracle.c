@@ -7,7 +7,7 @@
  * plasticity is always the exact return map applyPlasticity
  * (src/lib/gpu/shaderPrelude/plasticityOps.wgsl:7-48, restated in
  * mpm_oracle.c), which generates the training targets.  This file is the
- * checker of the GPU network's forward pass, its gradients and its strain-
+ * CPU reference of the GPU network's forward pass, its gradients and its strain-
  * bound check; only the tests load it.
  *
  * Two arithmetic modes:

@@ -7,7 +7,7 @@
  * src/lib/gpu/mpm/GpuMpmPipelineManager.ts:327-521).
  *
  * Only the test suite, the smoke check and the CPU-baseline leg of the
- * benchmark may load this code, and only as a checker or as the timed CPU
+ * benchmark may load this code, and only as the reference of a check or as the timed CPU
  * baseline.  The product library never links it.
  *
  * Parity status: UNPINNED.  The reference ships no golden vectors and its

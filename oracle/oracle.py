@@ -200,7 +200,7 @@ def aggregates(pos, vel, mass, Fp9):
     return com, mom, jp
 
 
-# ---- learned-plasticity network checker (mlp_oracle.c) ----------------
+# ---- learned-plasticity network reference (mlp_oracle.c) --------------
 MLP_PARAMS = 9867
 
 

@@ -1,4 +1,4 @@
-"""CPU checks of the learned-plasticity checker (oracle/mlp_oracle.c): its
+"""CPU checks of the learned-plasticity CPU reference (oracle/mlp_oracle.c): its
 backward pass against finite differences, the strain-bound check against the
 exact return map (plasticityOps.wgsl:7-48), and the training targets."""
 import numpy as np

@@ -1,5 +1,5 @@
-"""Learned plasticity on the GPU: the tensor-core network against the CPU
-checker (forward pass and gradients), the deferred exact pass against the
+"""Learned plasticity on the GPU: the tensor-core network against its CPU
+reference (forward pass and gradients), the deferred exact pass against the
 inline exact map (bit for bit), the collected training pairs against the
 exact return map, and the trained surrogate in a substep (accuracy of the
 aggregates against the f64 oracle, and what the trained network gains over
