@@ -984,7 +984,7 @@ def step_case(args, local):
 
     torch.cuda.set_device(local)
     pkg = importlib.import_module(PKG)
-    spec = build_scene(pkg, counts=args.counts)
+    spec = pkg.scenes.c1_pbmpm_spheres() if args.scene == "c1" else build_scene(pkg, counts=args.counts)
     n = spec.particles.shape[0]
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -1067,6 +1067,8 @@ def main():
                     help="skip the learned-plasticity and batched-scene legs (they run at N = 1 only)")
     ap.add_argument("--step-only", action="store_true",
                     help="run only warm-up + timed substeps of the slab (profiling case of the step's kernels)")
+    ap.add_argument("--scene", default="c2", choices=["c2", "c1"],
+                    help="--step-only: the slab (c2, default) or the two colliding spheres (c1)")
     ap.add_argument("--batched", action="store_true",
                     help="config 3 instead: 256 independent scenes sharded by scene over the ranks")
     ap.add_argument("--counts", default="256,64,256",

@@ -289,6 +289,73 @@ __global__ void k_tri_boxes(const uint32_t* __restrict__ col, uint32_t words, ui
     boxes[2 * t + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
 }
 
+// Squared distance from point p to triangle (a, b, c) in f64: the closest
+// point by the Voronoi-region walk of Ericson, "Real-Time Collision Detection"
+// (2005), section 5.1.5.
+__device__ double point_tri_dist2(const double* p, const double* a, const double* b, const double* c) {
+    double ab[3], ac[3], ap[3], q[3];
+    for (int k = 0; k < 3; k++) { ab[k] = b[k] - a[k]; ac[k] = c[k] - a[k]; ap[k] = p[k] - a[k]; }
+    auto dot = [](const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+    const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) {
+        for (int k = 0; k < 3; k++) q[k] = a[k];
+    } else {
+        double bp[3], cp[3];
+        for (int k = 0; k < 3; k++) { bp[k] = p[k] - b[k]; cp[k] = p[k] - c[k]; }
+        const double d3 = dot(ab, bp), d4 = dot(ac, bp), d5 = dot(ab, cp), d6 = dot(ac, cp);
+        const double vc = d1 * d4 - d3 * d2, vb = d5 * d2 - d1 * d6, va = d3 * d6 - d5 * d4;
+        if (d3 >= 0.0 && d4 <= d3) {
+            for (int k = 0; k < 3; k++) q[k] = b[k];
+        } else if (d6 >= 0.0 && d5 <= d6) {
+            for (int k = 0; k < 3; k++) q[k] = c[k];
+        } else if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+            const double v = d1 / (d1 - d3);
+            for (int k = 0; k < 3; k++) q[k] = a[k] + v * ab[k];
+        } else if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+            const double w = d2 / (d2 - d6);
+            for (int k = 0; k < 3; k++) q[k] = a[k] + w * ac[k];
+        } else if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+            const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+            for (int k = 0; k < 3; k++) q[k] = b[k] + w * (c[k] - b[k]);
+        } else {
+            const double den = 1.0 / (va + vb + vc);
+            const double v = vb * den, w = vc * den;
+            for (int k = 0; k < 3; k++) q[k] = a[k] + ab[k] * v + ac[k] * w;
+        }
+    }
+    double d[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+    return dot(d, d);
+}
+
+// One thread per cell of the res^3 field: the distance from the cell centre
+// to the nearest triangle (vertices read as the collider query reads them:
+// a word past the buffer reads as 0), minus half the cell diagonal and a
+// rounding allowance, rounded down to f32: a lower bound of the distance from
+// any point of the cell to every triangle (0 where it would be negative).
+__global__ void k_dist_field(const uint32_t* __restrict__ col, uint32_t words, uint32_t num_indices, double lo0,
+                             double lo1, double lo2, double cs0, double cs1, double cs2, uint32_t res,
+                             float* __restrict__ out) {
+    const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= res * res * res) return;
+    const uint32_t ix = cell % res, iy = (cell / res) % res, iz = cell / (res * res);
+    const double p[3] = {lo0 + (ix + 0.5) * cs0, lo1 + (iy + 0.5) * cs1, lo2 + (iz + 0.5) * cs2};
+    const uint32_t nt = num_indices / 3u;
+    double best = 1e300;
+    for (uint32_t t = 0; t < nt; t++) {
+        double v[3][3];
+        for (int j = 0; j < 3; j++) {
+            const size_t base = (size_t)num_indices + (size_t)__ldg(col + 3u * t + j) * 3u;
+            for (int k = 0; k < 3; k++)
+                v[j][k] = base + k < words ? (double)__uint_as_float(__ldg(col + base + k)) : 0.0;
+        }
+        best = fmin(best, point_tri_dist2(p, v[0], v[1], v[2]));
+    }
+    const double half = 0.5 * sqrt(cs0 * cs0 + cs1 * cs1 + cs2 * cs2);
+    const double mag = fmax(fmax(fabs(p[0]), fabs(p[1])), fabs(p[2]));
+    const double lb = sqrt(best) - half - 1e-6 * (1.0 + mag);
+    out[cell] = lb > 0.0 ? __double2float_rd(lb) : 0.0f;
+}
+
 uint32_t plan_nodes(uint32_t start, uint32_t count, uint32_t depth, std::vector<NodePlan>& out,
                     std::vector<uint32_t>& depth_of) {
     uint32_t id = (uint32_t)out.size();
@@ -410,6 +477,15 @@ cudaError_t triangle_boxes(const uint32_t* col_data, uint32_t words, uint32_t nu
     const uint32_t nt = num_indices / 3u;
     if (nt == 0) return cudaSuccess;
     bvhg::k_tri_boxes<<<(nt + 255) / 256, 256, 0, s>>>(col_data, words, num_indices, boxes);
+    return cudaGetLastError();
+}
+
+cudaError_t distance_field(const uint32_t* col_data, uint32_t words, uint32_t num_indices, const double* lo,
+                           const double* cs, uint32_t res, float* out, cudaStream_t s) {
+    const uint32_t n = res * res * res;
+    if (n == 0 || num_indices < 3) return cudaSuccess;
+    bvhg::k_dist_field<<<(n + 127) / 128, 128, 0, s>>>(col_data, words, num_indices, lo[0], lo[1], lo[2], cs[0],
+                                                       cs[1], cs[2], res, out);
     return cudaGetLastError();
 }
 

@@ -48,6 +48,8 @@ int bvh_build_device(const float* v, uint32_t nv, const uint32_t* idx, uint32_t 
                      uint32_t* order_dev, cudaStream_t s, cudaError_t* cuda_err);
 cudaError_t reorder_indices(const uint32_t* idx, const uint32_t* order, uint32_t nt, uint32_t* out, cudaStream_t s);
 cudaError_t triangle_boxes(const uint32_t* col_data, uint32_t words, uint32_t num_indices, float4* boxes, cudaStream_t s);
+cudaError_t distance_field(const uint32_t* col_data, uint32_t words, uint32_t num_indices, const double* lo,
+                           const double* cs, uint32_t res, float* out, cudaStream_t s);
 int mc_run(const uint32_t* density, const uint32_t* dres, const uint32_t* mres, const float* gmin, const float* gmax,
            float scale, float* out, uint32_t max_vertices, uint32_t* vertices_total, int n_sms, cudaStream_t s,
            cudaError_t* err);
@@ -73,7 +75,16 @@ struct SceneHost {
     uint32_t* col_data = nullptr;
     uint32_t* bvh = nullptr;
     float4* tbox = nullptr;   // per-triangle bounds (collide's early skip)
+    float* dfield = nullptr;  // distance field (collide's whole-query skip)
+    float df_lo[3] = {0.f, 0.f, 0.f}, df_rcs[3] = {0.f, 0.f, 0.f};
+    uint32_t df_res = 0;
 };
+
+// Distance field of a collider: DF_RES^3 cells over the triangles' bounds
+// widened by a tenth of their largest extent per side; built for meshes of at
+// most DF_MAX_TRIANGLES triangles (one thread per cell tests every triangle).
+constexpr uint32_t DF_RES = 32;
+constexpr uint32_t DF_MAX_TRIANGLES = 16384;
 
 struct MpmMlp {
     int device = 0;
@@ -310,6 +321,12 @@ static void build_scene_dev(SceneHost& s) {
         ident = ident && d.xf[i] == id && d.xfi[i] == id;
     }
     d.cull = (tbox && ident) ? 1u : 0u;
+    d.dfield = s.dfield;
+    for (int i = 0; i < 3; i++) {
+        d.df_lo[i] = s.df_lo[i];
+        d.df_rcs[i] = s.df_rcs[i];
+    }
+    d.df_res = s.dfield ? s.df_res : 0u;
     // Reciprocals RN(1/d) of the substep-constant divisors: one IEEE single
     // division each on the host, the value the oracle forms the same way.
     auto recip = [](float v) {
@@ -372,6 +389,7 @@ extern "C" int mpm_destroy(MpmHandle* h) {
         if (s.col_data) cudaFree(s.col_data);
         if (s.bvh) cudaFree(s.bvh);
         if (s.tbox) cudaFree(s.tbox);
+        if (s.dfield) cudaFree(s.dfield);
     }
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -648,6 +666,64 @@ extern "C" void* mpm_particles_device_ptr(MpmHandle* h) {
     return (void*)h->particles;
 }
 
+// (Re)builds scene s's distance field from its collider buffer and triangle
+// bounds (the stream is idle on entry and on return).  No field (and so no
+// whole-query skip) for meshes past DF_MAX_TRIANGLES or with non-finite bounds.
+static int build_field(MpmHandle* h, SceneHost& s, size_t words, uint32_t num_indices) {
+    if (s.dfield) { cudaFree(s.dfield); s.dfield = nullptr; }
+    s.df_res = 0;
+    const uint32_t nt = num_indices / 3u;
+    if (nt == 0 || nt > DF_MAX_TRIANGLES || !s.tbox || !s.col_data) return MPM_OK;
+    std::vector<float4> boxes((size_t)nt * 2);
+    CK(h, cudaMemcpy(boxes.data(), s.tbox, (size_t)nt * 32, cudaMemcpyDeviceToHost));
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (uint32_t t = 0; t < nt; t++) {
+        const float a[3] = {boxes[2 * t].x, boxes[2 * t].y, boxes[2 * t].z};
+        const float b[3] = {boxes[2 * t + 1].x, boxes[2 * t + 1].y, boxes[2 * t + 1].z};
+        for (int k = 0; k < 3; k++) {
+            if (!std::isfinite(a[k]) || !std::isfinite(b[k])) return MPM_OK;
+            lo[k] = std::min(lo[k], (double)a[k]);
+            hi[k] = std::max(hi[k], (double)b[k]);
+        }
+    }
+    const double ext = std::max(std::max(hi[0] - lo[0], hi[1] - lo[1]), std::max(hi[2] - lo[2], 1e-6));
+    double cs[3];
+    for (int k = 0; k < 3; k++) {
+        lo[k] -= 0.1 * ext;
+        hi[k] += 0.1 * ext;
+        cs[k] = (hi[k] - lo[k]) / DF_RES;
+    }
+    CK(h, cudaMalloc(&s.dfield, (size_t)DF_RES * DF_RES * DF_RES * 4));
+    CK(h, distance_field(s.col_data, (uint32_t)words, num_indices, lo, cs, DF_RES, s.dfield, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    // the query maps a position to cell floor((x - lo) * rcs): with lo and rcs
+    // rounded to f32 that may pick a neighbouring cell, so the stored bounds
+    // are each lowered to their 3^3 neighbourhood's minimum
+    std::vector<float> f((size_t)DF_RES * DF_RES * DF_RES), g(f.size());
+    CK(h, cudaMemcpy(f.data(), s.dfield, f.size() * 4, cudaMemcpyDeviceToHost));
+    const int R = (int)DF_RES;
+    for (int z = 0; z < R; z++)
+        for (int y = 0; y < R; y++)
+            for (int x = 0; x < R; x++) {
+                float m = f[((size_t)z * R + y) * R + x];
+                for (int dz = -1; dz <= 1; dz++)
+                    for (int dy = -1; dy <= 1; dy++)
+                        for (int dx = -1; dx <= 1; dx++) {
+                            const int X = x + dx, Y = y + dy, Z = z + dz;
+                            if (X < 0 || Y < 0 || Z < 0 || X >= R || Y >= R || Z >= R) continue;
+                            m = std::min(m, f[((size_t)Z * R + Y) * R + X]);
+                        }
+                g[((size_t)z * R + y) * R + x] = m;
+            }
+    CK(h, cudaMemcpy(s.dfield, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    s.df_res = DF_RES;
+    for (int k = 0; k < 3; k++) {
+        s.df_lo[k] = (float)lo[k];
+        s.df_rcs[k] = (float)(1.0 / cs[k]);
+    }
+    return MPM_OK;
+}
+
 extern "C" int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* data, size_t words, uint32_t num_indices,
                                 const void* nodes, uint32_t n_nodes) {
     int r = check_scene(h, scene);
@@ -672,6 +748,10 @@ extern "C" int mpm_set_collider(MpmHandle* h, uint32_t scene, const uint32_t* da
         CK(h, cudaMalloc(&s.tbox, (size_t)(num_indices / 3) * 32));
         CK(h, triangle_boxes(s.col_data, (uint32_t)words, num_indices, s.tbox, h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
+    }
+    {
+        int fr = build_field(h, s, words, num_indices);
+        if (fr) return fr;
     }
     s.dev.col_data = s.col_data;
     s.dev.bvh = s.bvh;
@@ -717,6 +797,8 @@ extern "C" int mpm_set_collider_mesh_device(MpmHandle* h, uint32_t scene, const 
     if (order) cudaFree(order);
     if (r == MPM_ERR_ARG) return fail(h, MPM_ERR_ARG, "mesh index >= n_vertices (%u)", n_vertices);
     if (r != MPM_OK || ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "device BVH build: %s", cudaGetErrorString(ce));
+    r = build_field(h, s, words, n_indices);
+    if (r) return r;
     s.dev.col_data = s.col_data;
     s.dev.bvh = s.bvh;
     s.dev.tbox = s.tbox;

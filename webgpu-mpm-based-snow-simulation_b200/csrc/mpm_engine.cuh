@@ -93,6 +93,13 @@ struct SceneDev {
     // its path are skipped (collide)
     const float4* tbox;
     uint32_t cull, cull_pad;
+    // distance field of the collider (used with the identity transform, as
+    // tbox): per cell of a df_res^3 grid over the triangles' bounds, a lower
+    // bound of the distance from any point of the cell to every triangle;
+    // nullptr when the collider has none
+    const float* dfield;
+    float df_lo[3], df_rcs[3];
+    uint32_t df_res, df_pad;
     // reciprocals RN(1/d) of the substep-constant divisors, rounded once on
     // the host: x / d evaluates as x * RN(1/d)
     float rdt, rcd[3], rscale, rfdiv;

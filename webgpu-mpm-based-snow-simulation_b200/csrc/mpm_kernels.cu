@@ -357,7 +357,8 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
     float hnorm[3] = {0.f, 0.f, 1.f}, hpos[3] = {cur[0], cur[1], cur[2]};
     bool has_hit = false;
     float rd[3] = {p.dxp[0], p.dxp[1], p.dxp[2]};
-    bool do_ccd = len3(rd) > 1e-4f;
+    const float rd_len = len3(rd);
+    bool do_ccd = rd_len > 1e-4f;
     float curl[3], prevl[3], pminl[3], pmaxl[3];
     xform_point(S.xfi, cur, curl);
     xform_point(S.xfi, prev, prevl);
@@ -372,6 +373,26 @@ __device__ void collide(const SceneDev& S, PState& p, Counters* ctr) {
     const float slack = fa(1e-4f, fm(1e-5f, fmaxf(fmaxf(fabsf(cur[0]), fabsf(cur[1])), fabsf(cur[2]))));
     const float reach = fa(S.cthr, slack);
     const float reach2 = fm(reach, reach);
+    // Whole-query skip (identity transform only): when the collider's
+    // distance field bounds the distance from the particle to every triangle
+    // from below by more than the threshold plus the path length, every point
+    // of the path is farther than the threshold from every triangle, so no
+    // triangle can bring the closest distance under the threshold and the path
+    // hits none: the query's outcome is "unchanged" without traversing.
+    if (S.cull && S.dfield != nullptr) {
+        bool in = true;
+        uint32_t fc[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float u = fm(fs(cur[k], S.df_lo[k]), S.df_rcs[k]);
+            in = in && u >= 0.f && u < (float)S.df_res;
+            fc[k] = in ? (uint32_t)u : 0u;
+        }
+        if (in && fc[0] < S.df_res && fc[1] < S.df_res && fc[2] < S.df_res) {
+            const float lb = __ldg(S.dfield + ((size_t)fc[2] * S.df_res + fc[1]) * S.df_res + fc[0]);
+            if (lb > fa(reach, rd_len)) return;
+        }
+    }
     float seg_lo[3], seg_hi[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
