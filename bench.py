@@ -460,7 +460,7 @@ def gpu_run(args, rank, world, local):
         "dtype": "f32 (fixed-point i32 grid)",
         "data": "synthetic (seeded procedural slab + fBm terrain; no dataset)",
         "config": bench_config(args.counts, args.steps, world),
-        "run": {"tile_edge": args.tile_edge, "occupied_tiles": n_tiles, "active_cells": n_cells,
+        "run": {"tile_edge": buf.tile_edge, "occupied_tiles": n_tiles, "active_cells": n_cells,
                 "n_iter": n_iter},
         "roofline": roofline,
         "p2g_gbs": round(p2g_gbs, 1),
@@ -871,7 +871,7 @@ def results_table(local):
         n = spec.particles.shape[0]
         method = spec.method
         # GPU throughput (state advanced by warm-up, graphs on)
-        buf, pipe = _pipeline(pkg, spec, 16, stream, local)
+        buf, pipe = _pipeline(pkg, spec, 0, stream, local)
         for _ in range(3):
             pipe.step(method, 1)
         buf.sync()
@@ -894,6 +894,7 @@ def results_table(local):
         grid = buf.dense_grid(spec.res, apply_grid_update=False)
         cells = int((grid[..., 0] != 0).sum())
         del grid
+        edge = buf.tile_edge
         buf.close()
         if method == 0:
             p2g = (n * (128 + 4) + cells * 16) / (kt["p2g_explicit"] * 1e-3) / 1e9
@@ -902,7 +903,7 @@ def results_table(local):
             p2g = (n * (12 + 4 + 36 + 36 + 12 + 36 + 4) + cells * 16) / (kt["pbmpm_first"] * 1e-3) / 1e9
             g2p = (cells * 16 + n * (4 + 88 + 144)) / (kt["g2p_pbmpm_integrate"] * 1e-3) / 1e9
         # GPU result after cmp_steps substeps from the initial state
-        buf, pipe = _pipeline(pkg, spec, 16, stream, local)
+        buf, pipe = _pipeline(pkg, spec, 0, stream, local)
         for _ in range(cmp_steps):
             pipe.step(method, 1)
         status = buf.sync()
@@ -922,7 +923,7 @@ def results_table(local):
                     for f in ("pos", "vel", "mass", "Fe", "Fp", "dxp", "D"))
         # GPU state after the configuration's own substep count, against the f64 oracle
         if agg_steps != cmp_steps:
-            buf, pipe = _pipeline(pkg, spec, 16, stream, local)
+            buf, pipe = _pipeline(pkg, spec, 0, stream, local)
             for _ in range(agg_steps):
                 pipe.step(method, 1)
             status |= buf.sync()
@@ -937,7 +938,7 @@ def results_table(local):
         o.close()
         err = _agg_rel_err(_agg(got), _agg_any(p64))
         rows.append({"config": name, "workload": spec.name, "particles": n, "method": "pbmpm" if method else "explicit",
-                     "gpu_value": gpu_rate, "gpu_steps": gpu_steps, "p2g_gbs": round(p2g, 1), "g2p_gbs": round(g2p, 1),
+                     "gpu_value": gpu_rate, "gpu_steps": gpu_steps, "tile_edge": edge, "p2g_gbs": round(p2g, 1), "g2p_gbs": round(g2p, 1),
                      "kernels_ms": {k: round(v, 4) for k, v in kt.items()}, "active_cells": cells,
                      "cpu_value": n * cmp_steps / cpu_s, "cpu_threads": threads, "cpu_steps": cmp_steps,
                      "bit_exact_vs_f32_oracle": bool(exact), "agg_steps": agg_steps, "agg_rel_err_vs_f64": err,
@@ -1012,7 +1013,8 @@ def step_case(args, local):
     lib.mpm_enable_kernel_timing(buf.handle, 0)
     names = pkg.kernel_names()
     kernels = {names[i]: round(kms[i] / kcnt[i], 4) for i in range(K) if kcnt[i]}
-    print(json.dumps({"case": "step", "particles": n, "tiles": buf.counts()[0], "ms_per_substep": ms,
+    print(json.dumps({"case": "step", "particles": n, "tiles": buf.counts()[0], "tile_edge": buf.tile_edge,
+                      "ms_per_substep": ms,
                       "value": n / (ms * 1e-3), "kernels_ms": kernels, "device_status": status}), flush=True)
     buf.close()
 
@@ -1056,7 +1058,8 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--tile-edge", type=int, default=16)
+    ap.add_argument("--tile-edge", type=int, default=0,
+                    help="grid tile edge 8, 12, 14 or 16; 0 lets the library choose from the occupied tiles")
     ap.add_argument("--cpu-steps", type=int, default=2,
                     help="timed substeps of the in-line CPU baseline (after one untimed substep)")
     ap.add_argument("--mlp-case", action="store_true",
@@ -1109,7 +1112,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.batched:
-        if args.tile_edge == 16:
+        if args.tile_edge == 0:
             args.tile_edge = 8   # the edge the autotuner picks for these scenes
         out = batched_sharded(args, rank, world, local)
         if rank == 0:

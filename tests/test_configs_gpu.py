@@ -189,3 +189,74 @@ def test_config3_batch_scenes_against_oracle(gpu, oracle_mod):
         o.close()
         compare_states(b.scene_particles(i, rec), want)
     b.close()
+
+
+def _tiles_at(gpu, spec, edge):
+    """Occupied tiles of the scene's first substep at a fixed tile edge."""
+    g = GpuScene(gpu, spec, tile_edge=edge)
+    assert g.step(1) == 0
+    n = g.buf.counts()[0]
+    g.close()
+    return n
+
+
+def _rule(n_st, n_sms, usable=(True, True, True)):
+    """The library's choice over edges (16, 12, 8): among the edges with at
+    least two occupied tiles per SM, the fewest halo cells ((E+2)^3 per tile;
+    a smaller edge only below 9/10 of the current choice's), else the edge
+    with the most tiles."""
+    edges = (16, 12, 8)
+    halo = [n * (e + 2) ** 3 for e, n in zip(edges, n_st)]
+    pick = None
+    for i in range(3):
+        if usable[i] and n_st[i] >= 2 * n_sms and (pick is None or 10 * halo[i] < 9 * halo[pick]):
+            pick = i
+    if pick is None:
+        pick = max((i for i in range(3) if usable[i]), key=lambda i: n_st[i])
+    return edges[pick]
+
+
+@pytest.mark.parametrize("name", ["c1", "c2_block"])
+def test_automatic_tile_edge_follows_occupancy_and_stays_bit_exact(gpu, oracle_mod, name):
+    """tile_edge 0: the first step picks the edge from the occupied tiles (two
+    spheres of config 1 fill 60 tiles of 16^3 and run at edge 8; the 524,288-
+    particle slab fills 676, whose halos hold fewer cells than its 1,620 tiles
+    of 12^3 or 4,732 of 8^3, and stays at 16); the substeps then equal the f32
+    oracle bit for bit."""
+    import torch
+
+    spec = SCENES[name](gpu)
+    n_sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n_st = [_tiles_at(gpu, spec, e) for e in (16, 12, 8)]
+    g = GpuScene(gpu, spec, tile_edge=0)
+    assert g.buf.tile_edge == 16          # nothing chosen before the first step
+    assert g.step(5) == 0
+    edge = g.buf.tile_edge
+    assert edge == _rule(n_st, n_sms), (n_st, edge)
+    assert edge == (8 if name == "c1" else 16)
+    got = g.particles()
+    g.close()
+    o, want = _oracle(oracle_mod, spec, 5)
+    o.close()
+    compare_states(got, want)
+
+
+def test_automatic_tile_edge_respects_fixed_max_tiles(gpu, oracle_mod):
+    """With a fixed tile capacity, an edge whose occupied tiles exceed it is
+    not a candidate: config 1 with room for 200 tiles runs at edge 12 (~100
+    tiles) instead of 8 (~240), bit-exact."""
+    import torch
+
+    spec = _c1(gpu)
+    n_sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n_st = [_tiles_at(gpu, spec, e) for e in (16, 12, 8)]
+    cap = 200
+    usable = [n <= cap for n in n_st]
+    g = GpuScene(gpu, spec, tile_edge=0, max_tiles=cap)
+    assert g.step(3) == 0
+    assert g.buf.tile_edge == _rule(n_st, n_sms, usable)
+    got = g.particles()
+    g.close()
+    o, want = _oracle(oracle_mod, spec, 3)
+    o.close()
+    compare_states(got, want)

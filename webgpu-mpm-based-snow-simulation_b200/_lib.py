@@ -122,6 +122,7 @@ SIGNATURES = {
     "mpm_step_p2g_only": (C.c_int, [_H, C.c_int]),
     "mpm_get_grid_dense": (C.c_int, [_H, C.c_uint32, C.c_int, C.c_void_p, C.c_size_t]),
     "mpm_get_counts": (C.c_int, [_H, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "mpm_get_tile_edge": (C.c_int, [_H, C.POINTER(C.c_uint32)]),
     "mpm_enable_kernel_timing": (C.c_int, [_H, C.c_int]),
     "mpm_set_schedule": (C.c_int, [_H, C.c_uint32, C.c_uint32]),
     "mpm_kernel_times": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_uint32]),

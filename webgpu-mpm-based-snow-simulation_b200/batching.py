@@ -52,7 +52,7 @@ def scene_aggregates(rec) -> list[float]:
     return [*map(float, com), *map(float, mom), abs_mom, jp]
 
 
-def advance_on_gpu(specs, method, steps: int, *, device: int = 0, tile_edge: int = 16, stream=None):
+def advance_on_gpu(specs, method, steps: int, *, device: int = 0, tile_edge: int = 0, stream=None):
     """Final records of each scene after `steps` substeps, all scenes in one
     GpuMpmBatch on `device` (the per-rank work of a sharded run)."""
     from .pipeline import GpuMpmBatch

@@ -112,6 +112,7 @@ struct MpmHandle {
     std::string err;
 
     uint32_t tile_edge = 16;
+    bool edge_auto = false;   // tile_edge 0 at creation: chosen by the first sizing pass
     uint32_t cap = 0;
     uint32_t max_tiles = 0;
     bool auto_tiles = true;   // tile capacity sized from the first binning, grown at sync points
@@ -439,6 +440,18 @@ static int alloc_tiles(MpmHandle* h, uint32_t n) {
     return MPM_OK;
 }
 
+// Makes `edge` the handle's tile edge: the tile kernels' shared-memory limits
+// and resident CTAs per SM for that edge.
+static int set_tile_edge(MpmHandle* h, uint32_t edge) {
+    cudaError_t ce = edge == 8u    ? configure_tile_kernels<8>(h->blocks_per_sm)
+                     : edge == 12u ? configure_tile_kernels<12>(h->blocks_per_sm)
+                     : edge == 14u ? configure_tile_kernels<14>(h->blocks_per_sm)
+                                   : configure_tile_kernels<16>(h->blocks_per_sm);
+    if (ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "configure kernels: %s", cudaGetErrorString(ce));
+    h->tile_edge = edge;
+    return MPM_OK;
+}
+
 extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     if (!cfg || !out) return MPM_ERR_ARG;
     *out = nullptr;
@@ -446,6 +459,7 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->cfg = *cfg;
     h->device = cfg->device;
     if (cfg->max_particles == 0) { *out = h; return fail(h, MPM_ERR_ARG, "max_particles must be > 0"); }
+    h->edge_auto = cfg->tile_edge == 0u;
     h->tile_edge = cfg->tile_edge ? cfg->tile_edge : 16u;
     if (h->tile_edge != 8u && h->tile_edge != 12u && h->tile_edge != 14u && h->tile_edge != 16u) {
         *out = h;
@@ -505,11 +519,10 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->n_scenes = 1;
     h->scene_first.assign(2, 0);
     h->n_particles = 0;
-    cudaError_t ce = h->tile_edge == 8u    ? configure_tile_kernels<8>(h->blocks_per_sm)
-                     : h->tile_edge == 12u ? configure_tile_kernels<12>(h->blocks_per_sm)
-                     : h->tile_edge == 14u ? configure_tile_kernels<14>(h->blocks_per_sm)
-                                           : configure_tile_kernels<16>(h->blocks_per_sm);
-    if (ce != cudaSuccess) return fail(h, MPM_ERR_CUDA, "configure kernels: %s", cudaGetErrorString(ce));
+    {
+        int r = set_tile_edge(h, h->tile_edge);
+        if (r) return r;
+    }
     CK(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
@@ -1021,10 +1034,11 @@ static int read_counters(MpmHandle* h, Counters* ct) {
 
 static uint32_t tiles_for(uint32_t n_st) { return std::max(1024u, n_st + n_st / 2u + 256u); }
 
-// Sizes the automatic capacities from a binning pass over the current
-// particles (no tile data is touched): the hash table to at least four slots
-// per occupied tile, the tile buffers to 1.5x the occupied tiles.
-static int size_from_binning(MpmHandle* h) {
+// One binning pass over the current particles at the handle's tile edge (no
+// tile data is touched), growing an automatic hash table until it holds four
+// slots per occupied tile.  *n_st gets the occupied tiles; *full is set when a
+// table of fixed capacity overflowed.
+static int binning_pass(MpmHandle* h, uint32_t* n_st, bool* full) {
     for (int attempt = 0; attempt < 4; attempt++) {
         Ctx c = make_ctx(h, h->work_cur);
         c.max_tiles = 0xFFFFFFFFu;  // no tile storage is touched by this pass
@@ -1035,8 +1049,8 @@ static int size_from_binning(MpmHandle* h) {
         Counters ct;
         int r = read_counters(h, &ct);
         if (r) return r;
-        bool full = (ct.status & ST_HASH_FULL) != 0u;
-        if (h->auto_cap && (full || ct.n_st * 4u > h->cap)) {
+        const bool over = (ct.status & ST_HASH_FULL) != 0u;
+        if (h->auto_cap && (over || ct.n_st * 4u > h->cap)) {
             uint32_t want = next_pow2(std::max(ct.n_st * 8u, h->cap * 4u));
             uint32_t z = 0;
             CK(h, cudaMemcpy(&h->counters->status, &z, 4, cudaMemcpyHostToDevice));
@@ -1044,14 +1058,86 @@ static int size_from_binning(MpmHandle* h) {
             if (r) return r;
             continue;
         }
-        if (full) return fail(h, MPM_ERR_CAPACITY, "tile hash table (%u slots) is full", h->cap);
-        if (h->auto_tiles && (h->tiles[0] == nullptr || ct.n_st > h->max_tiles)) {
-            r = alloc_tiles(h, tiles_for(ct.n_st));
-            if (r) return r;
-        }
+        *n_st = ct.n_st;
+        *full = over;
         return MPM_OK;
     }
     return fail(h, MPM_ERR_CAPACITY, "tile hash table could not be sized");
+}
+
+// Tile edge of a handle created with tile_edge 0, chosen once, from binning
+// passes of the current particles at edges 16, 12 and 8.  An edge qualifies
+// when its occupied tiles number at least two per SM (every SM has work and
+// the dynamic tile claiming can balance it).  Among the qualifying edges the
+// one whose tiles hold the fewest halo cells, (E+2)^3 per tile, is taken (the
+// per-particle work is the same at every edge; the halo assembly, conversion
+// and flush grow with the halo cells), a smaller edge only when it has under
+// 9/10 of the larger one's; when no edge qualifies, the edge with the most
+// tiles.  Edge 14 is not a candidate (its 16^3 halo buffer makes it slower
+// than both 12 and 16), nor is an edge whose tiles overflow a fixed hash
+// capacity or a fixed max_tiles.  Results do not depend on the edge.
+static int choose_tile_edge(MpmHandle* h) {
+    const uint32_t edges[3] = {16u, 12u, 8u};
+    uint32_t n_st[3] = {0u, 0u, 0u}, cap_at[3] = {0u, 0u, 0u};
+    bool usable[3] = {false, false, false};
+    for (int i = 0; i < 3; i++) {
+        int r = set_tile_edge(h, edges[i]);
+        if (r) return r;
+        bool full = false;
+        r = binning_pass(h, &n_st[i], &full);
+        if (r) return r;
+        cap_at[i] = h->cap;
+        usable[i] = !full && (h->auto_tiles || n_st[i] <= h->max_tiles);
+        if (full) {
+            // a fresh table and a clear status for the next candidate
+            uint32_t z = 0;
+            CK(h, cudaMemcpy(&h->counters->status, &z, 4, cudaMemcpyHostToDevice));
+            r = alloc_table(h, h->cap);
+            if (r) return r;
+        }
+    }
+    const uint32_t enough = 2u * (uint32_t)std::max(h->n_sms, 1);
+    auto halo_cells = [&](int i) {
+        const uint64_t hh = edges[i] + 2u;
+        return (uint64_t)n_st[i] * hh * hh * hh;
+    };
+    int pick = -1;
+    for (int i = 0; i < 3; i++)
+        if (usable[i] && n_st[i] >= enough && (pick < 0 || 10u * halo_cells(i) < 9u * halo_cells(pick))) pick = i;
+    if (pick < 0)
+        for (int i = 0; i < 3; i++)
+            if (usable[i] && (pick < 0 || n_st[i] > n_st[pick])) pick = i;
+    if (pick < 0) pick = 0;  // nothing fits: edge 16, whose sizing pass reports why
+    int r = set_tile_edge(h, edges[pick]);
+    if (r) return r;
+    // a table grown for a smaller edge's tiles is brought back to its size
+    if (h->auto_cap && h->cap > cap_at[pick]) {
+        r = alloc_table(h, cap_at[pick]);
+        if (r) return r;
+    }
+    h->edge_auto = false;
+    destroy_graphs(h);
+    return MPM_OK;
+}
+
+// Sizes the automatic capacities (and, for tile_edge 0, picks the tile edge)
+// from binning passes over the current particles: the hash table to at least
+// four slots per occupied tile, the tile buffers to 1.5x the occupied tiles.
+static int size_from_binning(MpmHandle* h) {
+    if (h->edge_auto) {
+        int r = choose_tile_edge(h);
+        if (r) return r;
+    }
+    uint32_t n_st = 0;
+    bool full = false;
+    int r = binning_pass(h, &n_st, &full);
+    if (r) return r;
+    if (full) return fail(h, MPM_ERR_CAPACITY, "tile hash table (%u slots) is full", h->cap);
+    if (h->auto_tiles && (h->tiles[0] == nullptr || n_st > h->max_tiles)) {
+        r = alloc_tiles(h, tiles_for(n_st));
+        if (r) return r;
+    }
+    return MPM_OK;
 }
 
 static int prepare_step(MpmHandle* h) {
@@ -1067,7 +1153,7 @@ static int prepare_step(MpmHandle* h) {
         h->work_valid = true;
         h->records_stale = false;
     }
-    if (h->tiles[0] == nullptr) {
+    if (h->tiles[0] == nullptr || h->edge_auto) {
         r = size_from_binning(h);
         if (r) return r;
     }
@@ -1086,6 +1172,7 @@ static uint64_t graph_signature(MpmHandle* h) {
         ((uint64_t)__builtin_bit_cast(uint32_t, h->det_threshold) << 32);
     s = s * 1315423911ull + (uint64_t)(uintptr_t)h->plast_list;
     s = s * 1315423911ull + (uint64_t)h->order_mode * 1024u + h->tile_block + (h->svd_any ? 7u : 0u);
+    s = s * 1315423911ull + h->tile_edge;
     return s | 1ull;
 }
 
@@ -1214,6 +1301,12 @@ extern "C" int mpm_get_counts(MpmHandle* h, uint32_t* n_tiles, uint32_t* n_binne
     CK(h, cudaMemcpy(&ct, h->counters, sizeof(ct), cudaMemcpyDeviceToHost));
     if (n_tiles) *n_tiles = ct.n_st;
     if (n_binned) *n_binned = ct.n_binned;
+    return MPM_OK;
+}
+
+extern "C" int mpm_get_tile_edge(MpmHandle* h, uint32_t* edge) {
+    if (!h || !edge) return MPM_ERR_ARG;
+    *edge = h->tile_edge;
     return MPM_OK;
 }
 

@@ -101,7 +101,7 @@ class GpuMpmBufferManager:
     sized from the particle count here instead of the reference's fixed
     500,000 blocks / 2,000,003 hash entries."""
 
-    def __init__(self, *, n_particles: int, device: int = 0, max_scenes: int = 1, tile_edge: int = 16,
+    def __init__(self, *, n_particles: int, device: int = 0, max_scenes: int = 1, tile_edge: int = 0,
                  max_tiles: int = 0, hash_capacity: int = 0, stream: int | None = None):
         lib = load()
         cfg = MpmConfig(max_particles=n_particles, max_scenes=max_scenes, max_tiles=max_tiles,
@@ -117,7 +117,6 @@ class GpuMpmBufferManager:
             self.handle = None
             raise _lib.MpmError(rc, msg)
         self.n_particles = n_particles
-        self.tile_edge = tile_edge
         self.device = device
         self._lib = lib
 
@@ -163,6 +162,14 @@ class GpuMpmBufferManager:
         a, b = C.c_uint32(0), C.c_uint32(0)
         check(self._lib.mpm_get_counts(self.handle, C.byref(a), C.byref(b)), self.handle)
         return a.value, b.value
+
+    @property
+    def tile_edge(self) -> int:
+        """The tile edge the substeps run with (tile_edge 0 at construction:
+        chosen by the first step from the occupied tiles, see mpm.h)."""
+        e = C.c_uint32(0)
+        check(self._lib.mpm_get_tile_edge(self.handle, C.byref(e)), self.handle)
+        return e.value
 
     def calculate_grid_mass(self, res, scene: int = 0, out=None):
         """calculateGridMass (GpuVolumetricRenderPipelineManager.ts): the mass
@@ -454,7 +461,7 @@ class GpuMpmBatch:
     kernel once over all tiles, captured in one CUDA graph.  The reference
     runs one scene per device; this is the batched form of its step."""
 
-    def __init__(self, specs, *, device: int = 0, tile_edge: int = 16, stream: int | None = None,
+    def __init__(self, specs, *, device: int = 0, tile_edge: int = 0, stream: int | None = None,
                  hash_capacity: int = 0, order_mode: int = 0, tile_block: int = 0):
         lib = load()
         self.specs = list(specs)
