@@ -46,7 +46,10 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms; start()
+    returns once the first sample arrived, begin()/end() mark the timed
+    region, and stop() summarises the samples that arrived inside it (all
+    samples when none did, with samples_in_region 0)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -55,28 +58,38 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
         self._t = None
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
         self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        deadline = time.monotonic() + 3.0
+        while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.monotonic()
+
+    def end(self):
+        self.t1 = time.monotonic()
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
+        time.sleep(0.1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -86,7 +99,9 @@ class ClockSampler:
             self._t.join(timeout=2)
         sm, mx, power, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        inside = [ln for t, ln in self.lines
+                  if self.t0 is not None and self.t1 is not None and self.t0 <= t <= self.t1 + 0.05]
+        for ln in inside or [ln for _, ln in self.lines]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -100,7 +115,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+                "power_w_max": max(power) if power else None, "samples": len(sm), "samples_in_region": len(inside),
+                "reasons": sorted(reasons)}
 
 
 def measured_peak_hbm():
@@ -225,12 +241,14 @@ def gpu_run(args, rank, world, local):
     clocks.start()
     barrier()
     torch.cuda.synchronize()
+    clocks.begin()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
         pipe.step(method, 1)
     ev1.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
@@ -756,12 +774,14 @@ def batched_sharded(args, rank, world, local):
     clocks.start()
     barrier()
     torch.cuda.synchronize()
+    clocks.begin()
     e0, e1 = _events(torch, stream)
     e0.record(stream)
     for _ in range(args.steps):
         b.step(method, 1)
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
