@@ -61,8 +61,8 @@ typedef struct MpmConfig {
     uint32_t max_tiles;      /* occupied grid tiles per substep (0: derived) */
     uint32_t hash_capacity;  /* tile hash slots, rounded up to a power of two (0: derived) */
     uint32_t tile_edge;      /* grid tile edge in cells: 8, 12, 14 or 16; 0: chosen at the
-                              * first step from the occupied tiles of the particles then
-                              * present (mpm_get_tile_edge) */
+                              * first step (and again after the particle count changes)
+                              * from the occupied tiles (mpm_get_tile_edge) */
     int32_t device;          /* CUDA device ordinal */
     void* stream;            /* cudaStream_t to order work on, or NULL for a private stream */
 } MpmConfig;
@@ -190,7 +190,8 @@ int mpm_get_grid_dense(MpmHandle* h, uint32_t scene, int apply_grid_update,
 int mpm_get_counts(MpmHandle* h, uint32_t* n_tiles, uint32_t* n_binned);
 /* The tile edge the substeps run with.  For a handle created with tile_edge 0
  * it is 16 until the first step picks one of 16, 12 and 8 from the occupied
- * tiles of the particles: among the edges with at least two occupied tiles per
+ * tiles of the particles (picked again by the first step after a change of
+ * the particle count): among the edges with at least two occupied tiles per
  * SM, the one whose tiles hold the fewest halo cells ((E+2)^3 per tile; a
  * smaller edge only below 9/10 of a larger one's), else the edge with the
  * most tiles.  Results do not depend on the tile edge. */

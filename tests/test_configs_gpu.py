@@ -16,7 +16,7 @@ the mean J_p (relative to itself) each within 1e-3.
 import numpy as np
 import pytest
 
-from helpers import GpuScene, compare_states
+from helpers import GpuScene, compare_states, make_params
 
 pytestmark = pytest.mark.gpu
 
@@ -260,3 +260,31 @@ def test_automatic_tile_edge_respects_fixed_max_tiles(gpu, oracle_mod):
     o, want = _oracle(oracle_mod, spec, 3)
     o.close()
     compare_states(got, want)
+
+
+def test_automatic_tile_edge_picked_again_for_a_new_particle_count(gpu, oracle_mod):
+    """One handle (tile_edge 0) first runs config 1 (edge 8), then is given the
+    524,288-particle slab: the next step picks edge 16, its tile buffers grow
+    to the larger halo, and the slab's substeps equal the f32 oracle bit for
+    bit."""
+    c1, slab = _c1(gpu), _c2_block(gpu)
+    n = max(c1.particles.shape[0], slab.particles.shape[0])
+    buf = gpu.GpuMpmBufferManager(n_particles=n, tile_edge=0)
+    try:
+        for spec, want_edge, steps in ((c1, 8, 2), (slab, 16, 3)):
+            buf.write_particles(spec.particles)
+            col = None
+            if spec.mesh is not None:
+                col = gpu.GpuColliderBufferManager(vertices=spec.mesh[0], indices=spec.mesh[1])
+            pipe = gpu.GpuMpmPipelineManager(mpm_manager=buf, uniforms_manager=spec.uniforms,
+                                             collider_manager=col, params=make_params(gpu, spec.params))
+            for _ in range(steps):
+                pipe.add_pbmpm_dispatches(n_particles=buf.n_particles)
+            assert buf.sync() == 0
+            assert buf.tile_edge == want_edge
+            got = buf.read_particles()
+            o, want = _oracle(oracle_mod, spec, steps)
+            o.close()
+            compare_states(got, want)
+    finally:
+        buf.close()

@@ -112,9 +112,11 @@ struct MpmHandle {
     std::string err;
 
     uint32_t tile_edge = 16;
-    bool edge_auto = false;   // tile_edge 0 at creation: chosen by the first sizing pass
+    bool edge_pick = false;   // created with tile_edge 0: the library picks the edge
+    bool edge_auto = false;   // the next sizing pass picks it (first step, new particle count)
     uint32_t cap = 0;
     uint32_t max_tiles = 0;
+    size_t tiles_nc = 0;      // halo cells per tile the tile buffers were sized for
     bool auto_tiles = true;   // tile capacity sized from the first binning, grown at sync points
     bool auto_cap = true;     // hash capacity grown at sync points
 
@@ -433,6 +435,7 @@ static int alloc_tiles(MpmHandle* h, uint32_t n) {
     if (h->tile_order) { cudaFree(h->tile_order); h->tile_order = nullptr; }
     size_t NC = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     h->max_tiles = n;
+    h->tiles_nc = NC;
     for (int i = 0; i < 3; i++) CK(h, cudaMalloc(&h->tiles[i], (size_t)n * NC * 16));
     CK(h, cudaMalloc(&h->st_nbr, (size_t)n * 27 * 4));
     CK(h, cudaMalloc(&h->tile_order, (size_t)n * 4));
@@ -459,7 +462,7 @@ extern "C" int mpm_create(const MpmConfig* cfg, MpmHandle** out) {
     h->cfg = *cfg;
     h->device = cfg->device;
     if (cfg->max_particles == 0) { *out = h; return fail(h, MPM_ERR_ARG, "max_particles must be > 0"); }
-    h->edge_auto = cfg->tile_edge == 0u;
+    h->edge_pick = h->edge_auto = cfg->tile_edge == 0u;
     h->tile_edge = cfg->tile_edge ? cfg->tile_edge : 16u;
     if (h->tile_edge != 8u && h->tile_edge != 12u && h->tile_edge != 14u && h->tile_edge != 16u) {
         *out = h;
@@ -584,6 +587,7 @@ static int set_count(MpmHandle* h, uint32_t n) {
     if (n != h->n_particles) {
         h->n_particles = n;
         h->work_valid = false;
+        h->edge_auto = h->edge_pick;  // a new particle count: the next step picks the edge again
         destroy_graphs(h);
         if (h->n_scenes == 1) {
             h->scenes[0].dev.p_first = 0;
@@ -1065,7 +1069,8 @@ static int binning_pass(MpmHandle* h, uint32_t* n_st, bool* full) {
     return fail(h, MPM_ERR_CAPACITY, "tile hash table could not be sized");
 }
 
-// Tile edge of a handle created with tile_edge 0, chosen once, from binning
+// Tile edge of a handle created with tile_edge 0, chosen at the first step
+// and again at the first step after the particle count changed, from binning
 // passes of the current particles at edges 16, 12 and 8.  An edge qualifies
 // when its occupied tiles number at least two per SM (every SM has work and
 // the dynamic tile claiming can balance it).  Among the qualifying edges the
@@ -1133,6 +1138,15 @@ static int size_from_binning(MpmHandle* h) {
     int r = binning_pass(h, &n_st, &full);
     if (r) return r;
     if (full) return fail(h, MPM_ERR_CAPACITY, "tile hash table (%u slots) is full", h->cap);
+    const size_t nc = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
+    if (h->tiles[0] != nullptr && h->tiles_nc < nc) {
+        // picked a larger edge than the buffers were sized for: the same tile
+        // count at the larger halo size
+        if (!h->auto_tiles && h->max_tiles < n_st)
+            return fail(h, MPM_ERR_CAPACITY, "%u occupied tiles > max_tiles %u", n_st, h->max_tiles);
+        r = alloc_tiles(h, h->auto_tiles ? tiles_for(n_st) : h->max_tiles);
+        if (r) return r;
+    }
     if (h->auto_tiles && (h->tiles[0] == nullptr || n_st > h->max_tiles)) {
         r = alloc_tiles(h, tiles_for(n_st));
         if (r) return r;

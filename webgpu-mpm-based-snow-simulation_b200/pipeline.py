@@ -166,7 +166,8 @@ class GpuMpmBufferManager:
     @property
     def tile_edge(self) -> int:
         """The tile edge the substeps run with (tile_edge 0 at construction:
-        chosen by the first step from the occupied tiles, see mpm.h)."""
+        chosen by the first step, and again after the particle count changes,
+        from the occupied tiles; see mpm.h)."""
         e = C.c_uint32(0)
         check(self._lib.mpm_get_tile_edge(self.handle, C.byref(e)), self.handle)
         return e.value
