@@ -57,6 +57,28 @@ def test_one_step_bit_exact(gpu, oracle_mod, kind, collider, interaction):
     g.close()
 
 
+@pytest.mark.parametrize("use_graphs", [True, False])
+@pytest.mark.parametrize("n_iter", [1, 2, 4, 5])
+def test_pbmpm_iteration_counts_bit_exact(gpu, oracle_mod, n_iter, use_graphs):
+    """PBMPM with 1 (no constraint iteration: the first transfer feeds G2P
+    directly), 2, 4 and 5 iterations, captured in graphs and launched eagerly:
+    particles after two substeps and the last transfer's grid (which of the
+    ping-pong buffers holds it depends on the count's parity) equal the
+    oracle's bit for bit."""
+    spec = _scene(gpu, kind="pbmpm", with_collider=True, n_iter=n_iter)
+    g = GpuScene(gpu, spec, use_graphs=use_graphs)
+    assert g.step(2) == 0
+    got = g.particles()
+    o, want = run_oracle(oracle_mod, spec, n_steps=2)
+    compare_states(got, want)
+    grid_gpu = g.grid()
+    grid_ref = o.dense_grid(spec.uniforms.bytes())
+    assert np.count_nonzero(grid_ref[..., 0]) > 100
+    assert np.array_equal(grid_gpu, grid_ref), f"{np.count_nonzero(grid_gpu != grid_ref)} cells differ"
+    o.close()
+    g.close()
+
+
 @pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
 def test_multi_step_bit_exact_and_aggregates(gpu, oracle_mod, kind):
     spec = _scene(gpu, kind=kind, with_collider=True, n_side=12)
