@@ -3,7 +3,7 @@ the same launches give each scene exactly the states it gets alone."""
 import numpy as np
 import pytest
 
-from helpers import GpuScene, compare_states
+from helpers import GpuScene, compare_states, run_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +37,31 @@ def test_batched_pbmpm_scenes_with_colliders_equal_solo_runs(gpu, tile_edge):
     rec = b.mpm.read_particles()
     for i, spec in enumerate(specs):
         compare_states(b.scene_particles(i, rec), _solo(gpu, spec, 3))
+    b.close()
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_batch_with_empty_scenes(gpu, oracle_mod, method):
+    """Scenes with no particles (first, middle and last in the buffer) leave
+    the others unchanged: each populated scene equals the f32 oracle's run of
+    it alone, bit for bit."""
+    import dataclasses
+
+    kind = "pbmpm" if method else "explicit"
+    full = [gpu.scenes.parity_scene(kind=kind, n_side=n, seed=s, with_collider=(method == 1))
+            for n, s in ((9, 50), (11, 51))]
+    empty = dataclasses.replace(full[0], particles=full[0].particles[:0].copy())
+    specs = [empty, full[0], empty, full[1], empty]
+    b = gpu.GpuMpmBatch(specs)
+    b.step(method, 3)
+    assert b.mpm.sync() == 0
+    rec = b.mpm.read_particles()
+    assert rec.shape[0] == sum(int(f.particles.shape[0]) for f in full)
+    for i, spec in ((1, full[0]), (3, full[1])):
+        o, want = run_oracle(oracle_mod, spec, n_steps=3)
+        o.close()
+        compare_states(b.scene_particles(i, rec), want)
+    assert b.scene_particles(0, rec).shape[0] == 0 and b.scene_particles(4, rec).shape[0] == 0
     b.close()
 
 

@@ -127,6 +127,25 @@ def test_small_and_ragged_counts(gpu, oracle_mod, n):
     g.close()
 
 
+@pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
+def test_coincident_particles_bit_exact(gpu, oracle_mod, kind):
+    """Half of the particles stacked on one point and a quarter on another
+    (every lane of a warp adding to the same grid cells): two substeps equal
+    the oracle bit for bit."""
+    spec = _scene(gpu, kind=kind, with_collider=(kind == "pbmpm"))
+    p = spec.particles
+    n = p.shape[0]
+    p["pos"][: n // 2] = p["pos"][0]
+    p["pos"][n // 2: 3 * n // 4] = p["pos"][n - 1]
+    g = GpuScene(gpu, spec)
+    assert g.step(2) == 0
+    got = g.particles()
+    o, want = run_oracle(oracle_mod, spec, n_steps=2)
+    o.close()
+    compare_states(got, want)
+    g.close()
+
+
 @pytest.mark.parametrize("kind", ["pbmpm", "explicit"])
 def test_tile_edges_agree(gpu, oracle_mod, kind):
     spec = _scene(gpu, kind=kind, with_collider=True)
