@@ -60,7 +60,8 @@ using namespace mpm;
 static const char* kKernelNames[K_COUNT] = {
     "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
     "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense",
-    "tile_nbr", "plasticity", "tile_order", "p2g_explicit_b128", "g2p_explicit_integrate_b128"};
+    "tile_nbr", "plasticity", "tile_order", "p2g_explicit_b128", "g2p_explicit_integrate_b128", "pbmpm_iter_wide",
+    "pbmpm_first_wide", "g2p_pbmpm_integrate_wide"};
 
 struct TimedLaunch {
     uint32_t kid;
@@ -171,6 +172,7 @@ struct MpmHandle {
 
     int blocks_per_sm[K_COUNT] = {0};
 
+    bool iter_wide = false;       // 512-thread PBMPM iteration CTAs (tile edge 8, few tiles)
     uint32_t order_mode = 0;      // schedule knobs (mpm_set_schedule)
     uint32_t tile_block = 0;
     bool use_graphs = true;
@@ -1008,7 +1010,7 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
         uint32_t n_iter = h->scenes[0].params.n_iter;
         int cur = 0;
         c.tiles_a = h->tiles[cur];
-        L(K_PBMPM_FIRST);
+        L(h->iter_wide ? K_PBMPM_FIRST_WIDE : K_PBMPM_FIRST);
         if (stop_p2g) { h->last_tiles = cur; return cudaSuccess; }
         for (uint32_t it = 1; it < n_iter; it++) {
             int nxt = cur == 1 ? 2 : 1;
@@ -1016,13 +1018,13 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
             c.tiles_a = h->tiles[nxt];
             c.iter_first = it == 1 ? 1u : 0u;
             c.order_rev = it & 1u;
-            L(K_PBMPM_ITER);
+            L(h->iter_wide ? K_PBMPM_ITER_WIDE : K_PBMPM_ITER);
             cur = nxt;
         }
         c.tiles_b = h->tiles[cur];
         c.g2p_rm = n_iter > 1 ? 1u : 0u;
         c.order_rev = n_iter & 1u;
-        L(K_G2P_PBMPM);
+        L(h->iter_wide ? K_G2P_PBMPM_WIDE : K_G2P_PBMPM);
         if (h->plast_mode != PLAST_INLINE || h->svd_any) L(K_PLASTICITY);
         h->last_tiles = cur;
     }
@@ -1138,6 +1140,10 @@ static int size_from_binning(MpmHandle* h) {
     int r = binning_pass(h, &n_st, &full);
     if (r) return r;
     if (full) return fail(h, MPM_ERR_CAPACITY, "tile hash table (%u slots) is full", h->cap);
+    // At tile edge 8 with fewer than two occupied tiles per SM a launch lasts
+    // about as long as its heaviest tile: the iterations then run 512-thread
+    // CTAs (one per SM), which finish a tile's particles in half the rounds.
+    h->iter_wide = h->tile_edge == 8u && n_st < 2u * (uint32_t)std::max(h->n_sms, 1);
     const size_t nc = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);
     if (h->tiles[0] != nullptr && h->tiles_nc < nc) {
         // picked a larger edge than the buffers were sized for: the same tile
@@ -1186,7 +1192,7 @@ static uint64_t graph_signature(MpmHandle* h) {
         ((uint64_t)__builtin_bit_cast(uint32_t, h->det_threshold) << 32);
     s = s * 1315423911ull + (uint64_t)(uintptr_t)h->plast_list;
     s = s * 1315423911ull + (uint64_t)h->order_mode * 1024u + h->tile_block + (h->svd_any ? 7u : 0u);
-    s = s * 1315423911ull + h->tile_edge;
+    s = s * 1315423911ull + h->tile_edge * 2u + (h->iter_wide ? 1u : 0u);
     return s | 1ull;
 }
 

@@ -214,6 +214,9 @@ enum KernelId : uint32_t {
     K_TILE_ORDER,
     K_P2G_EXPLICIT_128,       // the explicit tile kernels with 128-thread CTAs (schedule knob)
     K_G2P_EXPLICIT_128,
+    K_PBMPM_ITER_WIDE,        // the PBMPM tile kernels with 512-thread CTAs at tile edge 8 (few tiles)
+    K_PBMPM_FIRST_WIDE,
+    K_G2P_PBMPM_WIDE,
     K_COUNT
 };
 

@@ -1933,8 +1933,11 @@ size_t smem_bytes(uint32_t kid) {
         case K_G2P_EXPLICIT:
         case K_G2P_PBMPM:
         case K_P2G_EXPLICIT_128:
-        case K_G2P_EXPLICIT_128: return 16 * NC;
-        case K_PBMPM_ITER: return 32 * NC;
+        case K_G2P_EXPLICIT_128:
+        case K_PBMPM_FIRST_WIDE:
+        case K_G2P_PBMPM_WIDE: return 16 * NC;
+        case K_PBMPM_ITER:
+        case K_PBMPM_ITER_WIDE: return 32 * NC;
         default: return 0;
     }
 }
@@ -1945,6 +1948,8 @@ constexpr int iter_block() { return E == 16 ? 512 : 256; }
 template <int E>
 int block_size(uint32_t kid) {
     if (kid == K_P2G_EXPLICIT_128 || kid == K_G2P_EXPLICIT_128) return 128;
+    if (kid == K_PBMPM_ITER_WIDE) return E == 8 ? 512 : iter_block<E>();
+    if (kid == K_PBMPM_FIRST_WIDE || kid == K_G2P_PBMPM_WIDE) return E == 8 ? 512 : BS_DEFAULT;
     return kid == K_PBMPM_ITER ? iter_block<E>() : BS_DEFAULT;
 }
 
@@ -1960,6 +1965,29 @@ int kernel_ptrs(uint32_t kid, void** out) {
             out[0] = (void*)k_pbmpm_iter<E, iter_block<E>(), true>;
             out[1] = (void*)k_pbmpm_iter<E, iter_block<E>(), false>;
             return 2;
+        case K_PBMPM_ITER_WIDE:
+            if constexpr (E == 8) {
+                out[0] = (void*)k_pbmpm_iter<E, 512, true>;
+                out[1] = (void*)k_pbmpm_iter<E, 512, false>;
+                return 2;
+            } else {
+                return kernel_ptrs<E>(K_PBMPM_ITER, out);
+            }
+        case K_PBMPM_FIRST_WIDE:
+            if constexpr (E == 8) {
+                out[0] = (void*)k_pbmpm_first<E, 512>;
+                return 1;
+            } else {
+                return kernel_ptrs<E>(K_PBMPM_FIRST, out);
+            }
+        case K_G2P_PBMPM_WIDE:
+            if constexpr (E == 8) {
+                out[0] = (void*)k_g2p_integrate<E, true, 512, 2>;
+                out[1] = (void*)k_g2p_integrate<E, true, 512, 0>;
+                return 2;
+            } else {
+                return kernel_ptrs<E>(K_G2P_PBMPM, out);
+            }
         case K_G2P_PBMPM:
             out[0] = (void*)k_g2p_integrate<E, true, BS_DEFAULT, 2>;
             out[1] = (void*)k_g2p_integrate<E, true, BS_DEFAULT, 0>;
@@ -1975,7 +2003,8 @@ int kernel_ptrs(uint32_t kid, void** out) {
 template <int E>
 cudaError_t configure_tile_kernels(int* blocks_per_sm) {
     for (uint32_t kid : {K_P2G_EXPLICIT, K_G2P_EXPLICIT, K_PBMPM_FIRST, K_PBMPM_ITER, K_G2P_PBMPM, K_GRID_DENSE,
-                         K_P2G_EXPLICIT_128, K_G2P_EXPLICIT_128}) {
+                         K_P2G_EXPLICIT_128, K_G2P_EXPLICIT_128, K_PBMPM_ITER_WIDE, K_PBMPM_FIRST_WIDE,
+                         K_G2P_PBMPM_WIDE}) {
         void* fs[2] = {nullptr, nullptr};
         int nf = kernel_ptrs<E>(kid, fs);
         size_t sm = smem_bytes<E>(kid);
@@ -2013,6 +2042,26 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
         case K_PBMPM_ITER:
             if (c.iter_first) k_pbmpm_iter<E, iter_block<E>(), true><<<grid_tiles, iter_block<E>(), smem_bytes<E>(kid), s>>>(c);
             else k_pbmpm_iter<E, iter_block<E>(), false><<<grid_tiles, iter_block<E>(), smem_bytes<E>(kid), s>>>(c);
+            break;
+        case K_PBMPM_ITER_WIDE:
+            if constexpr (E == 8) {
+                if (c.iter_first) k_pbmpm_iter<E, 512, true><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+                else k_pbmpm_iter<E, 512, false><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+            } else {
+                return launch_kernel<E>(K_PBMPM_ITER, c, s, grid_tiles, scene, apply, out);
+            }
+            break;
+        case K_PBMPM_FIRST_WIDE:
+            if constexpr (E == 8) k_pbmpm_first<E, 512><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+            else return launch_kernel<E>(K_PBMPM_FIRST, c, s, grid_tiles, scene, apply, out);
+            break;
+        case K_G2P_PBMPM_WIDE:
+            if constexpr (E == 8) {
+                if (c.g2p_rm) k_g2p_integrate<E, true, 512, 2><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+                else k_g2p_integrate<E, true, 512, 0><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+            } else {
+                return launch_kernel<E>(K_G2P_PBMPM, c, s, grid_tiles, scene, apply, out);
+            }
             break;
         case K_G2P_PBMPM:
             if (c.g2p_rm) k_g2p_integrate<E, true, BS_DEFAULT, 2><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c);
