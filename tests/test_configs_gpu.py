@@ -290,13 +290,14 @@ def test_automatic_tile_edge_picked_again_for_a_new_particle_count(gpu, oracle_m
         buf.close()
 
 
-def test_edge8_iteration_widths_bit_exact(gpu, oracle_mod):
-    """At tile edge 8 the PBMPM tile kernels (first transfer, iterations, G2P)
-    run 512-thread CTAs when the occupied tiles number fewer than two per SM
-    (config 1: 248 tiles) and their usual widths otherwise (the 524,288-
-    particle slab: 4,732 tiles); both equal the f32 oracle bit for bit after
-    two substeps."""
+def test_edge8_tile_kernel_widths_bit_exact(gpu, oracle_mod):
+    """At tile edge 8 the tile kernels run 512-thread CTAs when the occupied
+    tiles number fewer than two per SM (config 1: 248 tiles; config 0: 80) and
+    their usual widths otherwise (the 524,288-particle slab: 4,732 tiles),
+    for PBMPM (first transfer, iterations, G2P) and explicit MPM (P2G, G2P);
+    every case equals the f32 oracle bit for bit after two substeps."""
     import ctypes as C
+    import dataclasses
 
     import torch
 
@@ -304,7 +305,12 @@ def test_edge8_iteration_widths_bit_exact(gpu, oracle_mod):
     names = gpu.kernel_names()
     K = lib.mpm_kernel_count()
     n_sms = torch.cuda.get_device_properties(0).multi_processor_count
-    for spec in (_c1(gpu), _c2_block(gpu)):
+    slab = _c2_block(gpu)
+    cases = [(_c1(gpu), ("pbmpm_first", 2), ("pbmpm_iter", 2 * 5), ("g2p_pbmpm_integrate", 2)),
+             (slab, ("pbmpm_first", 2), ("pbmpm_iter", 2 * 5), ("g2p_pbmpm_integrate", 2)),
+             (_c0(gpu), ("p2g_explicit", 2), ("g2p_explicit_integrate", 2)),
+             (dataclasses.replace(slab, method=0), ("p2g_explicit", 2), ("g2p_explicit_integrate", 2))]
+    for spec, *expect in cases:
         g = GpuScene(gpu, spec, tile_edge=8)
         lib.mpm_enable_kernel_timing(g.buf.handle, 1)
         assert g.step(2) == 0
@@ -312,9 +318,9 @@ def test_edge8_iteration_widths_bit_exact(gpu, oracle_mod):
         lib.mpm_kernel_times(g.buf.handle, kms, kcnt, K)
         launches = {names[i]: kcnt[i] for i in range(K) if kcnt[i]}
         wide = g.buf.counts()[0] < 2 * n_sms
-        for k, n in (("pbmpm_first", 2), ("pbmpm_iter", 2 * 5), ("g2p_pbmpm_integrate", 2)):
+        for k, n in expect:
             used, unused = (k + "_wide", k) if wide else (k, k + "_wide")
-            assert launches.get(used, 0) == n and unused not in launches, launches
+            assert launches.get(used, 0) == n and unused not in launches, (spec.name, launches)
         got = g.particles()
         g.close()
         o, want = _oracle(oracle_mod, spec, 2)

@@ -61,7 +61,7 @@ static const char* kKernelNames[K_COUNT] = {
     "clear_table", "bin_insert", "compact_a", "compact_b", "compact_c", "bin_scatter",
     "p2g_explicit", "g2p_explicit_integrate", "pbmpm_first", "pbmpm_iter", "g2p_pbmpm_integrate", "grid_dense",
     "tile_nbr", "plasticity", "tile_order", "p2g_explicit_b128", "g2p_explicit_integrate_b128", "pbmpm_iter_wide",
-    "pbmpm_first_wide", "g2p_pbmpm_integrate_wide"};
+    "pbmpm_first_wide", "g2p_pbmpm_integrate_wide", "p2g_explicit_wide", "g2p_explicit_integrate_wide"};
 
 struct TimedLaunch {
     uint32_t kid;
@@ -172,7 +172,7 @@ struct MpmHandle {
 
     int blocks_per_sm[K_COUNT] = {0};
 
-    bool iter_wide = false;       // 512-thread PBMPM iteration CTAs (tile edge 8, few tiles)
+    bool iter_wide = false;       // 512-thread tile-kernel CTAs (tile edge 8, few tiles)
     uint32_t order_mode = 0;      // schedule knobs (mpm_set_schedule)
     uint32_t tile_block = 0;
     bool use_graphs = true;
@@ -995,13 +995,16 @@ static cudaError_t enqueue_substep(MpmHandle* h, int method, int parity, bool ca
     // before it (which wrote the tiles it reads)
     c.order_rev = 0u;
     if (method == MPM_METHOD_EXPLICIT) {
+        // CTA width: the schedule knob, else 512 threads for few tiles at edge 8
         const bool b128 = h->tile_block == 128u;
+        const uint32_t k_p2g = b128 ? K_P2G_EXPLICIT_128 : h->iter_wide ? K_P2G_EXPLICIT_WIDE : K_P2G_EXPLICIT;
+        const uint32_t k_g2p = b128 ? K_G2P_EXPLICIT_128 : h->iter_wide ? K_G2P_EXPLICIT_WIDE : K_G2P_EXPLICIT;
         c.tiles_a = h->tiles[0];
-        L(b128 ? K_P2G_EXPLICIT_128 : K_P2G_EXPLICIT);
+        L(k_p2g);
         if (stop_p2g) { h->last_tiles = 0; return cudaSuccess; }
         c.tiles_b = h->tiles[0];
         c.order_rev = 1u;
-        L(b128 ? K_G2P_EXPLICIT_128 : K_G2P_EXPLICIT);
+        L(k_g2p);
         if (h->plast_mode != PLAST_INLINE || h->svd_any) L(K_PLASTICITY);
         h->last_tiles = 0;
     } else {
@@ -1141,7 +1144,7 @@ static int size_from_binning(MpmHandle* h) {
     if (r) return r;
     if (full) return fail(h, MPM_ERR_CAPACITY, "tile hash table (%u slots) is full", h->cap);
     // At tile edge 8 with fewer than two occupied tiles per SM a launch lasts
-    // about as long as its heaviest tile: the iterations then run 512-thread
+    // about as long as its heaviest tile: the tile kernels then run 512-thread
     // CTAs (one per SM), which finish a tile's particles in half the rounds.
     h->iter_wide = h->tile_edge == 8u && n_st < 2u * (uint32_t)std::max(h->n_sms, 1);
     const size_t nc = (size_t)(h->tile_edge + 2) * (h->tile_edge + 2) * (h->tile_edge + 2);

@@ -217,6 +217,8 @@ enum KernelId : uint32_t {
     K_PBMPM_ITER_WIDE,        // the PBMPM tile kernels with 512-thread CTAs at tile edge 8 (few tiles)
     K_PBMPM_FIRST_WIDE,
     K_G2P_PBMPM_WIDE,
+    K_P2G_EXPLICIT_WIDE,      // the explicit tile kernels with 512-thread CTAs at tile edge 8 (few tiles)
+    K_G2P_EXPLICIT_WIDE,
     K_COUNT
 };
 

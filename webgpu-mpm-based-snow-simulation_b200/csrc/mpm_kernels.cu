@@ -1935,7 +1935,9 @@ size_t smem_bytes(uint32_t kid) {
         case K_P2G_EXPLICIT_128:
         case K_G2P_EXPLICIT_128:
         case K_PBMPM_FIRST_WIDE:
-        case K_G2P_PBMPM_WIDE: return 16 * NC;
+        case K_G2P_PBMPM_WIDE:
+        case K_P2G_EXPLICIT_WIDE:
+        case K_G2P_EXPLICIT_WIDE: return 16 * NC;
         case K_PBMPM_ITER:
         case K_PBMPM_ITER_WIDE: return 32 * NC;
         default: return 0;
@@ -1949,7 +1951,9 @@ template <int E>
 int block_size(uint32_t kid) {
     if (kid == K_P2G_EXPLICIT_128 || kid == K_G2P_EXPLICIT_128) return 128;
     if (kid == K_PBMPM_ITER_WIDE) return E == 8 ? 512 : iter_block<E>();
-    if (kid == K_PBMPM_FIRST_WIDE || kid == K_G2P_PBMPM_WIDE) return E == 8 ? 512 : BS_DEFAULT;
+    if (kid == K_PBMPM_FIRST_WIDE || kid == K_G2P_PBMPM_WIDE || kid == K_P2G_EXPLICIT_WIDE ||
+        kid == K_G2P_EXPLICIT_WIDE)
+        return E == 8 ? 512 : BS_DEFAULT;
     return kid == K_PBMPM_ITER ? iter_block<E>() : BS_DEFAULT;
 }
 
@@ -1988,6 +1992,20 @@ int kernel_ptrs(uint32_t kid, void** out) {
             } else {
                 return kernel_ptrs<E>(K_G2P_PBMPM, out);
             }
+        case K_P2G_EXPLICIT_WIDE:
+            if constexpr (E == 8) {
+                out[0] = (void*)k_p2g_explicit<E, 512>;
+                return 1;
+            } else {
+                return kernel_ptrs<E>(K_P2G_EXPLICIT, out);
+            }
+        case K_G2P_EXPLICIT_WIDE:
+            if constexpr (E == 8) {
+                out[0] = (void*)k_g2p_integrate<E, false, 512, 0>;
+                return 1;
+            } else {
+                return kernel_ptrs<E>(K_G2P_EXPLICIT, out);
+            }
         case K_G2P_PBMPM:
             out[0] = (void*)k_g2p_integrate<E, true, BS_DEFAULT, 2>;
             out[1] = (void*)k_g2p_integrate<E, true, BS_DEFAULT, 0>;
@@ -2004,7 +2022,7 @@ template <int E>
 cudaError_t configure_tile_kernels(int* blocks_per_sm) {
     for (uint32_t kid : {K_P2G_EXPLICIT, K_G2P_EXPLICIT, K_PBMPM_FIRST, K_PBMPM_ITER, K_G2P_PBMPM, K_GRID_DENSE,
                          K_P2G_EXPLICIT_128, K_G2P_EXPLICIT_128, K_PBMPM_ITER_WIDE, K_PBMPM_FIRST_WIDE,
-                         K_G2P_PBMPM_WIDE}) {
+                         K_G2P_PBMPM_WIDE, K_P2G_EXPLICIT_WIDE, K_G2P_EXPLICIT_WIDE}) {
         void* fs[2] = {nullptr, nullptr};
         int nf = kernel_ptrs<E>(kid, fs);
         size_t sm = smem_bytes<E>(kid);
@@ -2062,6 +2080,14 @@ cudaError_t launch_kernel(uint32_t kid, const Ctx& c, cudaStream_t s, int grid_t
             } else {
                 return launch_kernel<E>(K_G2P_PBMPM, c, s, grid_tiles, scene, apply, out);
             }
+            break;
+        case K_P2G_EXPLICIT_WIDE:
+            if constexpr (E == 8) k_p2g_explicit<E, 512><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+            else return launch_kernel<E>(K_P2G_EXPLICIT, c, s, grid_tiles, scene, apply, out);
+            break;
+        case K_G2P_EXPLICIT_WIDE:
+            if constexpr (E == 8) k_g2p_integrate<E, false, 512, 0><<<grid_tiles, 512, smem_bytes<E>(kid), s>>>(c);
+            else return launch_kernel<E>(K_G2P_EXPLICIT, c, s, grid_tiles, scene, apply, out);
             break;
         case K_G2P_PBMPM:
             if (c.g2p_rm) k_g2p_integrate<E, true, BS_DEFAULT, 2><<<grid_tiles, BS_DEFAULT, smem_bytes<E>(kid), s>>>(c);
