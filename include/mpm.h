@@ -101,8 +101,12 @@ typedef struct MpmParams {
 int mpm_default_params(MpmParams* out);
 /* Allocates the particle and bookkeeping buffers.  Grid-tile storage and the
  * tile hash table are sized from the first substep's occupancy when
- * max_tiles / hash_capacity are 0, and grown only inside mpm_sync (between
- * substeps); a substep itself never allocates. */
+ * max_tiles / hash_capacity are 0 (again by the first step after the particle
+ * count changes) and grown only inside mpm_sync (between substeps); a substep
+ * itself never allocates.  Records of the same count that occupy many more tiles than the
+ * previous ones can exceed the storage in the first substep after them: it
+ * sets MPM_STATUS_TILE_OVERFLOW (or HASH_FULL) and leaves the particles of the
+ * tiles beyond the storage unchanged, and the next mpm_sync grows it. */
 int mpm_create(const MpmConfig* cfg, MpmHandle** out);
 int mpm_destroy(MpmHandle* h);
 const char* mpm_last_error(const MpmHandle* h);

@@ -262,16 +262,19 @@ def test_automatic_tile_edge_respects_fixed_max_tiles(gpu, oracle_mod):
     compare_states(got, want)
 
 
-def test_automatic_tile_edge_picked_again_for_a_new_particle_count(gpu, oracle_mod):
-    """One handle (tile_edge 0) first runs config 1 (edge 8), then is given the
-    524,288-particle slab: the next step picks edge 16, its tile buffers grow
-    to the larger halo, and the slab's substeps equal the f32 oracle bit for
-    bit."""
+@pytest.mark.parametrize("tile_edge,edges", [(0, (8, 16)), (8, (8, 8))])
+def test_new_particle_count_sizes_the_handle_again(gpu, oracle_mod, tile_edge, edges):
+    """One handle first runs config 1, then is given the 524,288-particle slab
+    (a new particle count): the next step sizes the tile storage again (at
+    edge 8 the slab fills 4,732 tiles, against 248 for config 1) and, with
+    tile_edge 0, picks the edge again (8, then 16, the tile buffers growing to
+    the larger halo); no capacity status is raised and the slab's substeps
+    equal the f32 oracle bit for bit."""
     c1, slab = _c1(gpu), _c2_block(gpu)
     n = max(c1.particles.shape[0], slab.particles.shape[0])
-    buf = gpu.GpuMpmBufferManager(n_particles=n, tile_edge=0)
+    buf = gpu.GpuMpmBufferManager(n_particles=n, tile_edge=tile_edge)
     try:
-        for spec, want_edge, steps in ((c1, 8, 2), (slab, 16, 3)):
+        for spec, want_edge, steps in ((c1, edges[0], 2), (slab, edges[1], 3)):
             buf.write_particles(spec.particles)
             col = None
             if spec.mesh is not None:
@@ -326,3 +329,51 @@ def test_edge8_tile_kernel_widths_bit_exact(gpu, oracle_mod):
         o, want = _oracle(oracle_mod, spec, 2)
         o.close()
         compare_states(got, want)
+
+
+def test_edge8_width_follows_the_tile_count_at_sync(gpu, oracle_mod):
+    """The CTA width at tile edge 8 follows the occupied tiles at each sync:
+    a handle with fixed tile storage starts at the usual width, turns wide
+    after the first sync of config 1 (248 tiles), and back after the sync that
+    follows new records spread over the whole domain (thousands of tiles);
+    the spread particles' substeps equal the f32 oracle bit for bit."""
+    import ctypes as C
+
+    lib = gpu.load()
+    names = gpu.kernel_names()
+    K = lib.mpm_kernel_count()
+
+    def launches(h):
+        kms, kcnt = (C.c_float * K)(), (C.c_uint32 * K)()
+        lib.mpm_kernel_times(h, kms, kcnt, K)
+        lib.mpm_enable_kernel_timing(h, 1)     # and start counting again
+        return {names[i]: kcnt[i] for i in range(K) if kcnt[i]}
+
+    spec = _c1(gpu)
+    g = GpuScene(gpu, spec, tile_edge=8, max_tiles=8192)
+    h = g.buf.handle
+    lib.mpm_enable_kernel_timing(h, 1)
+    assert g.step(1) == 0
+    assert launches(h).get("pbmpm_iter") == 5
+    assert g.step(1) == 0
+    assert launches(h).get("pbmpm_iter_wide") == 5
+    spread = spec.particles.copy()
+    rng = np.random.default_rng(3)
+    spread["pos"] = rng.uniform(0.05, 0.95, spread["pos"].shape).astype(np.float32)
+    g.buf.write_particles(spread)
+    assert g.step(1) == 0
+    assert launches(h).get("pbmpm_iter_wide") == 5
+    import torch
+    assert g.buf.counts()[0] >= 3 * torch.cuda.get_device_properties(0).multi_processor_count
+    assert g.step(2) == 0
+    last = launches(h)
+    assert last.get("pbmpm_iter") == 10 and "pbmpm_iter_wide" not in last, last
+    got = g.particles()
+    g.close()
+    o = oracle_mod.Oracle(spread.shape[0], max_blocks=600000, hash_size=2000003)
+    o.set_collider(*spec.mesh)
+    want = spread.copy()
+    for _ in range(3):
+        o.step(spec.uniforms.bytes(), spec.params, want, spec.method)
+    o.close()
+    compare_states(got, want)

@@ -115,6 +115,7 @@ struct MpmHandle {
     uint32_t tile_edge = 16;
     bool edge_pick = false;   // created with tile_edge 0: the library picks the edge
     bool edge_auto = false;   // the next sizing pass picks it (first step, new particle count)
+    bool sizing_due = false;  // a new particle count: the next step sizes automatic storage again
     uint32_t cap = 0;
     uint32_t max_tiles = 0;
     size_t tiles_nc = 0;      // halo cells per tile the tile buffers were sized for
@@ -590,6 +591,7 @@ static int set_count(MpmHandle* h, uint32_t n) {
         h->n_particles = n;
         h->work_valid = false;
         h->edge_auto = h->edge_pick;  // a new particle count: the next step picks the edge again
+        h->sizing_due = h->auto_tiles && h->auto_cap;
         destroy_graphs(h);
         if (h->n_scenes == 1) {
             h->scenes[0].dev.p_first = 0;
@@ -1176,9 +1178,10 @@ static int prepare_step(MpmHandle* h) {
         h->work_valid = true;
         h->records_stale = false;
     }
-    if (h->tiles[0] == nullptr || h->edge_auto) {
+    if (h->tiles[0] == nullptr || h->edge_auto || h->sizing_due) {
         r = size_from_binning(h);
         if (r) return r;
+        h->sizing_due = false;
     }
     return MPM_OK;
 }
@@ -1284,6 +1287,16 @@ extern "C" int mpm_sync(MpmHandle* h, uint32_t* status_out) {
     if (h->auto_cap && ct.n_st * 4u > h->cap) {
         r = alloc_table(h, next_pow2(ct.n_st * 8u));
         if (r) return r;
+    }
+    // the CTA width of the tile kernels follows the occupied tiles (with a
+    // margin, so a count near the limit does not switch it at every sync)
+    if (h->tile_edge == 8u && h->tiles[0]) {
+        const uint32_t s = (uint32_t)std::max(h->n_sms, 1);
+        const bool wide = h->iter_wide ? ct.n_st < 3u * s : ct.n_st < 2u * s;
+        if (wide != h->iter_wide) {
+            h->iter_wide = wide;
+            destroy_graphs(h);
+        }
     }
     if (ct.status) return fail(h, MPM_ERR_DEVICE_STATUS, "device status 0x%x", ct.status);
     return MPM_OK;
