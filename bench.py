@@ -713,15 +713,15 @@ def batched_leg(pkg, args, local, stream):
     method = pkg.GpuSimulationMethodType.ExplicitMpm
     n_total = int(sum(s.particles.shape[0] for s in specs))
     sched, times = pkg.batching.autotune_schedule(specs, method, steps=3, device=local)
-    best = sched["tile_edge"]
     b = pkg.GpuMpmBatch(specs, device=local, stream=stream.cuda_stream, **sched)
     steps = max(10, min(args.steps, 30))
     ms = pkg.batching.time_batch(b, method, steps, warmup=3)
     b.close()
-    # the plain per-scene loop: one handle per scene, launched one after another
+    # the plain per-scene loop: one handle per scene (each at the tile edge the
+    # library picks for it), launched one after another
     handles = []
     for spec in specs:
-        buf, pipe = _pipeline(pkg, spec, best, stream, local)
+        buf, pipe = _pipeline(pkg, spec, 0, stream, local)
         handles.append((buf, pipe))
     for buf, pipe in handles:
         pipe.step(method, 2)
