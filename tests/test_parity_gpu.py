@@ -57,16 +57,18 @@ def test_one_step_bit_exact(gpu, oracle_mod, kind, collider, interaction):
     g.close()
 
 
+@pytest.mark.parametrize("tile_edge", [16, 8])
 @pytest.mark.parametrize("use_graphs", [True, False])
 @pytest.mark.parametrize("n_iter", [1, 2, 4, 5])
-def test_pbmpm_iteration_counts_bit_exact(gpu, oracle_mod, n_iter, use_graphs):
+def test_pbmpm_iteration_counts_bit_exact(gpu, oracle_mod, n_iter, use_graphs, tile_edge):
     """PBMPM with 1 (no constraint iteration: the first transfer feeds G2P
-    directly), 2, 4 and 5 iterations, captured in graphs and launched eagerly:
-    particles after two substeps and the last transfer's grid (which of the
-    ping-pong buffers holds it depends on the count's parity) equal the
-    oracle's bit for bit."""
+    directly), 2, 4 and 5 iterations, captured in graphs and launched eagerly,
+    at tile edge 16 and at edge 8 (where this small scene's few tiles run the
+    512-thread tile kernels): particles after two substeps and the last
+    transfer's grid (which of the ping-pong buffers holds it depends on the
+    count's parity) equal the oracle's bit for bit."""
     spec = _scene(gpu, kind="pbmpm", with_collider=True, n_iter=n_iter)
-    g = GpuScene(gpu, spec, use_graphs=use_graphs)
+    g = GpuScene(gpu, spec, tile_edge=tile_edge, use_graphs=use_graphs)
     assert g.step(2) == 0
     got = g.particles()
     o, want = run_oracle(oracle_mod, spec, n_steps=2)
