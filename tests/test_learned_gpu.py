@@ -60,13 +60,15 @@ def _scene(gpu, kind, seed=10, n_side=16):
     return gpu.scenes.parity_scene(kind=kind, n_side=n_side, seed=seed, with_collider=True)
 
 
+@pytest.mark.parametrize("tile_edge", [16, 8])
 @pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
-def test_deferred_exact_equals_inline(gpu, kind):
+def test_deferred_exact_equals_inline(gpu, kind, tile_edge):
     """The strain-bound check plus a separate exact pass reproduces the
-    inline exact map bit for bit, over several substeps with yielding."""
+    inline exact map bit for bit, over several substeps with yielding (at
+    edge 8 this small scene runs the 512-thread tile kernels)."""
     spec = _scene(gpu, kind)
-    a = GpuScene(gpu, spec)
-    b = GpuScene(gpu, spec)
+    a = GpuScene(gpu, spec, tile_edge=tile_edge)
+    b = GpuScene(gpu, spec, tile_edge=tile_edge)
     ctl = gpu.learned.PlasticityController(b.buf)
     ctl.set_mode(gpu._lib.PLASTICITY_EXACT)
     assert a.step(6) == 0 and b.step(6) == 0
@@ -77,15 +79,16 @@ def test_deferred_exact_equals_inline(gpu, kind):
     b.close()
 
 
+@pytest.mark.parametrize("tile_edge", [16, 8])
 @pytest.mark.parametrize("kind", ["explicit", "pbmpm"])
-def test_svd_return_map_bit_exact(gpu, oracle_mod, kind):
+def test_svd_return_map_bit_exact(gpu, oracle_mod, kind, tile_edge):
     """The SVD return map (return_map 1, an option of this library, applied by
     the deferred plasticity pass) equals the oracle's restatement bit for
-    bit over several substeps with yielding; it is a different map from the
-    reference's (the states differ)."""
+    bit over several substeps with yielding, at tile edges 16 and 8; it is a
+    different map from the reference's (the states differ)."""
     spec = _scene(gpu, kind)
     spec.params["return_map"] = 1
-    g = GpuScene(gpu, spec)
+    g = GpuScene(gpu, spec, tile_edge=tile_edge)
     assert g.step(4) == 0
     got = g.particles()
     g.close()
